@@ -1,0 +1,448 @@
+#!/usr/bin/env python
+"""D'D CG time-to-solution on a 32^3 x 64 Wilson-clover lattice on B200.
+
+One step = one complete D'D conjugate-gradient solve, zero start, to FP64 true
+relative residual 1e-10 (benchmark/ddagd_cg/ddagd_cg.jl:587-664 protocol),
+mixed precision: int16-storage / FP32-arithmetic inner D'D with FP64 reliable
+updates (delta 0.1).  The plain FP64 CG (the reference's algorithm and
+arithmetic, cg.jl:73-137) is timed in the same run for the "mixed vs FP64"
+comparison.  Inputs: SU(3) links exp(0.2 i H), H Gaussian traceless Hermitian
+(seed 1), reunitarized; unit-variance complex Gaussian source (seed 2);
+kappa 0.1355, cSW 1.0, phases (1,1,1,-1).  Everything synthetic; the links
+(1.2 GB) and clover blocks exceed the 126 MB L2, so no flush is needed.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+N > 1 (torchrun): every rank solves its own replica (the path has no data
+exchange at one GPU per lattice); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "latticematrices.jl_b200"))
+
+METRIC = ("D†D CG time-to-1e-10 mixed vs FP64, Dslash HBM GB/s; "
+          "32³×64 clover, 1 B200")
+PHASES = (1, 1, 1, -1)
+
+# Plain FP64 CG iterations this workload needs (32^3x64, kappa 0.1355,
+# cSW 1.0, links exp(0.2 i H) seed 1, source seed 2, rtol 1e-10), measured by
+# the GPU FP64 solve of this file; the CPU reference arm multiplies its
+# per-iteration time by it.
+FP64_ITERATIONS_32x64 = None
+
+# Algorithmic bytes per lattice site of the two stencil kernels of a CG
+# iteration: every operand read once, every output written once.
+#  K1  tmp = D p  (+|tmp|^2):  links 4x18 reals, clover 2x36 reals, p, tmp
+#  K2  D^+ tmp fused with x += a p, r -= a Ap, |r|^2:  links, clover, tmp,
+#      p, r (read+write), x (read+write, FP32 for the mixed solves)
+SPINOR_BYTES = {"double": 192, "single": 96, "half": 52}   # 24 reals (+norm)
+GAUGE_BYTES = {"double": 576 + 576, "single": 288 + 288, "half": 144 + 144}
+X_BYTES = {"double": 192, "single": 96, "half": 96}
+
+
+def k1_bytes(prec):
+    return GAUGE_BYTES[prec] + 2 * SPINOR_BYTES[prec]
+
+
+def k2_bytes(prec):
+    return GAUGE_BYTES[prec] + 4 * SPINOR_BYTES[prec] + 2 * X_BYTES[prec]
+
+
+# Wilson-clover M: 1320 (hopping) + 504 (clover) + 48 flops per site
+FLOPS_PER_SITE_M = 1872
+
+
+def parse():
+    ap = argparse.ArgumentParser(description=__doc__,
+                                 formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["lmb", "reference"], default="lmb")
+    ap.add_argument("--lattice", default="32,32,32,64")
+    ap.add_argument("--precision", default="half", choices=["single", "half"])
+    ap.add_argument("--kappa", type=float, default=0.1355)
+    ap.add_argument("--csw", type=float, default=1.0)
+    ap.add_argument("--amplitude", type=float, default=0.2)
+    ap.add_argument("--rtol", type=float, default=1e-10)
+    ap.add_argument("--delta", type=float, default=0.1)
+    ap.add_argument("--maxiter", type=int, default=20000)
+    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-clocks", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (one process per GPU)
+# ---------------------------------------------------------------------------
+def dist_setup(backend):
+    import torch.distributed as dist
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws > 1 and not dist.is_initialized():
+        from datetime import timedelta
+        dist.init_process_group(backend, timeout=timedelta(seconds=600))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, local, ws
+
+
+def max_over_ranks(value, ws, device=None):
+    if ws == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,"
+              "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap")
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle's FP64 CG on the same workload, bounded sample
+# ---------------------------------------------------------------------------
+def cpu_fp64_cg_seconds_per_iteration(L, kappa, csw, amplitude, budget_s):
+    from oracle import oracle as orc
+    orc.build()
+    threads = os.cpu_count() or 1
+    orc.set_num_threads(threads)
+    U = orc.random_su3_links(L, amplitude, 1)
+    b = orc.gaussian_field(L, 3, 4, 2)
+    F = orc.clover_field_strength(U)
+    op = orc.Operator(orc.OP_CLOVER, U, L, kappa=kappa, csw=csw, F=F)
+    t1 = orc.cg_iterations_seconds(op, b, 1)
+    n = max(1, int(budget_s / max(t1, 1e-3)))
+    tn = orc.cg_iterations_seconds(op, b, n)
+    return tn / n, n, orc.num_threads()
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def traffic_per_site():
+    """DRAM bytes per site per launch from a committed ncu capture summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "dslash_traffic.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+# ---------------------------------------------------------------------------
+# arms
+# ---------------------------------------------------------------------------
+def run_reference(args):
+    rank, _, ws = dist_setup("gloo")
+    if rank != 0:
+        return
+    L = tuple(int(v) for v in args.lattice.split(","))
+    sites = L[0] * L[1] * L[2] * L[3]
+    from oracle import oracle as orc
+    orc.build()
+    threads = os.cpu_count() or 1
+    orc.set_num_threads(threads)
+    U = orc.random_su3_links(L, args.amplitude, 1)
+    b = orc.gaussian_field(L, 3, 4, 2)
+    F = orc.clover_field_strength(U)
+    op = orc.Operator(orc.OP_CLOVER, U, L, kappa=args.kappa, csw=args.csw, F=F)
+    for _ in range(args.warmup):
+        orc.cg_iterations_seconds(op, b, 1)
+    per = []
+    for _ in range(args.steps):
+        per.append(orc.cg_iterations_seconds(op, b, 1))
+    t_iter = statistics.mean(per)
+    iters = FP64_ITERATIONS_32x64 if L == (32, 32, 32, 64) else None
+    value = t_iter * iters if iters else t_iter
+    unit = "s" if iters else "s/iteration"
+    sample = (f"{args.steps} FP64 CG iterations (D'D clover + BLAS) on the "
+              f"full {L} lattice after {args.warmup} warm-up iterations; "
+              f"value = mean seconds per iteration x {iters} iterations "
+              f"(the FP64 iteration count of this workload)"
+              if iters else "seconds per FP64 CG iteration")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": unit,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_iter * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "Wilson-clover D'D CG, FP64, CPU oracle port "
+                   "of the reference algorithm", "lattice": list(L),
+                   "sites": sites, "kappa": args.kappa, "csw": args.csw},
+        "cpu_baseline": {"value": value, "unit": unit, "cores": threads,
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_lmb(args):
+    import numpy as np
+    import torch
+
+    rank, local, ws = dist_setup("nccl")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    import lmb200 as lmb
+
+    L = tuple(int(v) for v in args.lattice.split(","))
+    sites = L[0] * L[1] * L[2] * L[3]
+    U = lmb.random_su3_links(L, args.amplitude, 1, nw=1, device=dev)
+    b = lmb.gaussian_fermion(L, 3, 4, 2, nw=1, phases=PHASES, device=dev)
+    D = lmb.WilsonDiracCloverOperator4D(U, args.kappa, args.csw)
+    A = lmb.DdagDOp(D, b.similar())
+    x = b.similar()
+    stream = torch.cuda.current_stream()
+
+    def solve(prec, profile=False):
+        lmb.clear_matrix_(x)
+        return lmb.cg_(x, A, b, rtol=args.rtol, maxiter=args.maxiter,
+                       precision=prec, delta=args.delta, profile=profile)
+
+    def true_rel():
+        t1, t2 = b.similar(), b.similar()
+        lmb.mul_(t1, D, x)
+        lmb.mul_(t2, lmb.adjoint(D), t1)
+        r = b.core_view() - t2.core_view()
+        return float(torch.linalg.vector_norm(r) / torch.linalg.vector_norm(b.core_view()))
+
+    prec = args.precision
+    # warm-up (builds link/clover caches, JIT-free)
+    for _ in range(args.warmup):
+        solve(prec)
+    solve("double")
+
+    # ---- timed: mixed precision solves (value) ----
+    results = []
+    barrier(ws)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    if args.no_clocks:
+        clocks.proc = None
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with (clocks if not args.no_clocks else _Null()):
+        start.record(stream)
+        for _ in range(args.steps):
+            results.append(solve(prec, profile=True))
+        end.record(stream)
+        torch.cuda.synchronize()
+    barrier(ws)
+    t_mixed = start.elapsed_time(end) / 1e3 / args.steps
+    t_mixed = max_over_ranks(t_mixed, ws, dev)
+    mixed_true = true_rel()
+    mixed = results[-1]
+
+    # ---- timed: plain FP64 CG (the reference's arithmetic) ----
+    r64 = []
+    barrier(ws)
+    torch.cuda.synchronize()
+    start.record(stream)
+    for _ in range(args.fp64_steps):
+        r64.append(solve("double", profile=True))
+    end.record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    t_fp64 = max_over_ranks(start.elapsed_time(end) / 1e3 / args.fp64_steps, ws, dev)
+    fp64_true = true_rel()
+    res64 = r64[-1]
+
+    # ---- e2e: host buffers, copies inside the timed region ----
+    b_host = b.A.cpu().pin_memory()
+    x_host = torch.empty_like(b_host).pin_memory()
+    e2e_t = []
+    barrier(ws)
+    torch.cuda.synchronize()
+    start.record(stream)
+    for _ in range(args.steps):
+        b.A.copy_(b_host, non_blocking=True)
+        lmb.mark_halo_dirty_(b)
+        solve(prec)
+        x_host.copy_(x.A, non_blocking=True)
+    end.record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    t_e2e = max_over_ranks(start.elapsed_time(end) / 1e3 / args.steps, ws, dev)
+    nbytes = b_host.numel() * b_host.element_size()
+
+    # ---- roofline of the dominant stencil kernel (mixed solve) ----
+    k1_ms = sum(r.dslash_ms for r in results)
+    k2_ms = sum(r.update_ms for r in results)
+    k1_n = sum(r.dslash_launches for r in results)
+    k2_n = sum(r.update_launches for r in results)
+    peak, peak_kind = measured_peak()
+    dominant = "K2 (D^+ tmp fused with the CG update)" if k2_ms >= k1_ms \
+        else "K1 (tmp = D p with |tmp|^2)"
+    if k2_ms >= k1_ms:
+        per_launch_ms, bps = k2_ms / max(k2_n, 1), k2_bytes(prec)
+        tkey = f"k2_{prec}"
+    else:
+        per_launch_ms, bps = k1_ms / max(k1_n, 1), k1_bytes(prec)
+        tkey = f"k1_{prec}"
+    achieved = bps * sites / (per_launch_ms * 1e-3) / 1e9
+    traffic = traffic_per_site().get(tkey)
+    k1_gbs = k1_bytes(prec) * sites / (k1_ms / max(k1_n, 1) * 1e-3) / 1e9
+    k2_gbs = k2_bytes(prec) * sites / (k2_ms / max(k2_n, 1) * 1e-3) / 1e9
+    k1_64 = sum(r.dslash_ms for r in r64) / max(sum(r.dslash_launches for r in r64), 1)
+    k2_64 = sum(r.update_ms for r in r64) / max(sum(r.update_launches for r in r64), 1)
+    gbs64 = k1_bytes("double") * sites / (k1_64 * 1e-3) / 1e9
+    gflops = lambda ms: FLOPS_PER_SITE_M * sites / (ms * 1e-3) / 1e9
+
+    line = {
+        "metric": METRIC, "value": t_mixed, "unit": "s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_mixed * 1e3,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 arithmetic on int16 storage, f64 reliable updates"
+        if prec == "half" else "f32 inner, f64 reliable updates",
+        "data": "synthetic",
+        "config": {
+            "workload": ("Wilson-clover D'D CG to FP64 true residual "
+                         f"{args.rtol:g}, {L[0]}x{L[1]}x{L[2]}x{L[3]}, "
+                         f"kappa {args.kappa}, cSW {args.csw}, links "
+                         f"exp({args.amplitude} i H) seed 1, Gaussian source "
+                         "seed 2, zero start"),
+            "lattice": list(L), "sites": sites, "inner_precision": prec,
+            "reliable_delta": args.delta,
+            "l2": "inputs larger than L2 (links 1.2 GB + clover), no flush",
+            "parallelism": f"replicas x{ws}",
+        },
+        "mixed": {"time_s": t_mixed, "iterations": mixed.iterations,
+                  "reliable_updates": mixed.reliable_updates,
+                  "true_rel_residual": mixed_true},
+        "fp64": {"time_s": t_fp64, "iterations": res64.iterations,
+                 "true_rel_residual": fp64_true},
+        "speedup_mixed_vs_fp64": t_fp64 / t_mixed,
+        "dslash": {
+            "fp64_k1_gbs": gbs64, "fp64_k1_gflops_M": gflops(k1_64),
+            "fp64_k1_ms": k1_64, "fp64_k2_ms": k2_64,
+            f"{prec}_k1_gbs": k1_gbs, f"{prec}_k2_gbs": k2_gbs,
+            f"{prec}_k1_ms": k1_ms / max(k1_n, 1),
+            f"{prec}_k2_ms": k2_ms / max(k2_n, 1),
+            f"{prec}_k1_gflops_M": gflops(k1_ms / max(k1_n, 1)),
+        },
+        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved,
+                     "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": achieved / peak,
+                     "bytes_per_site": bps,
+                     "traffic": traffic * sites if traffic else None},
+        "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": nbytes,
+                "d2h_bytes_per_step": nbytes},
+        "gpu_launches": int(sum(r.kernel_launches for r in results)),
+    }
+    if not args.no_clocks:
+        line["clocks"] = clocks.summary()
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        t_iter, n, cores = cpu_fp64_cg_seconds_per_iteration(
+            L, args.kappa, args.csw, args.amplitude, args.cpu_seconds)
+        line["cpu_baseline"] = {
+            "value": t_iter * res64.iterations, "unit": "s", "cores": cores,
+            "kind": "port",
+            "sample": (f"{n} FP64 CG iterations of the oracle on the full "
+                       f"lattice ({t_iter:.3f} s each) x {res64.iterations} "
+                       "iterations of the FP64 solve")}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        return False
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_lmb(args)
+
+
+if __name__ == "__main__":
+    main()

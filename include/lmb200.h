@@ -1,0 +1,166 @@
+/*
+ * lmb200.h -- C ABI of liblmb200.so, the B200 (sm_100a) implementation of the
+ * LatticeMatrices.jl Dirac-operator hot path.
+ *
+ * Plain C types only: device pointers are `void *` to the reference's
+ * halo-padded field storage (the CuArray behind a LatticeMatrix, column-major
+ * (NC1, NC2, X+2nw, Y+2nw, Z+2nw, T+2nw), LatticeMatrices_core.jl:4-9,
+ * 361-363), streams are `void *` (cudaStream_t; NULL = legacy default
+ * stream).  Every call writes only the core sites of its outputs; the caller
+ * marks the output halo dirty exactly as _parallel_for_mutating! does
+ * (LatticeMatrices_core.jl:216-219).
+ *
+ * Errors: every int-returning entry point returns LMB_OK (0) or a negative
+ * LMB_ERR_* code and never traps or throws; lmb_last_error() holds the text.
+ * Threading: one context per host thread / stream; a context is not
+ * re-entrant.  Calls are ordered on the caller's stream; only lmb_cg_ddagd and
+ * lmb_field_dot synchronise with the host, as the reference's `cg!` and `dot`
+ * return host scalars.
+ */
+#ifndef LMB200_H
+#define LMB200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LMB_OK 0
+#define LMB_ERR_ARG (-1)         /* validation failure (ArgumentError)     */
+#define LMB_ERR_CUDA (-2)        /* CUDA runtime error                     */
+#define LMB_ERR_STATE (-3)       /* geometry or links not set              */
+#define LMB_ERR_UNSUPPORTED (-4) /* combination not provided by this build */
+
+#define LMB_DTYPE_C128 0 /* ComplexF64 fields */
+#define LMB_DTYPE_C64 1  /* ComplexF32 fields */
+
+#define LMB_PREC_DOUBLE 0 /* FP64 storage and arithmetic                       */
+#define LMB_PREC_SINGLE 1 /* FP32 storage and arithmetic                       */
+#define LMB_PREC_HALF 2   /* int16 storage (per-site norm), FP32 arithmetic    */
+
+#define LMB_OP_WILSON 0
+#define LMB_OP_WILSON_CLOVER 1
+#define LMB_OP_STAGGERED 2
+#define LMB_OP_HISQ 3
+
+#define LMB_LINKS_THIN 0 /* Wilson / clover / staggered links U_mu      */
+#define LMB_LINKS_FAT 1  /* HISQ fat links X_mu (HISQLinks4D)           */
+#define LMB_LINKS_LONG 2 /* HISQ Naik links L_mu (HISQLinks4D)          */
+
+/* CG status, mirroring CGResult.reason (LinearAlgebras/cg.jl:1-13) */
+#define LMB_CG_CONVERGED 0
+#define LMB_CG_MAXIMUM_ITERATIONS 1
+#define LMB_CG_NONPOSITIVE_CURVATURE 2
+#define LMB_CG_NUMERICAL_BREAKDOWN 3
+
+typedef struct lmb_ctx lmb_ctx;
+
+typedef struct {
+  int op;              /* LMB_OP_*                                              */
+  double kappa, csw;   /* Wilson / Wilson-clover                                */
+  double mass;         /* staggered / HISQ                                      */
+  double naik_epsilon; /* HISQ                                                  */
+  double rtol, atol;   /* stop when |r| <= max(atol, rtol |b|) (cg.jl:61-63)    */
+  int maxiter;
+  int precision;       /* LMB_PREC_DOUBLE: plain FP64 CG (cg.jl:73-137);
+                          SINGLE / HALF: inner D'D at that precision with FP64
+                          reliable updates and an FP64 true-residual stop        */
+  double delta;        /* reliable-update threshold (mixed only), e.g. 0.1      */
+  int check_interval;  /* iterations between host status checks (0 = default)  */
+  int profile;         /* 1: time every stencil launch with CUDA events        */
+} lmb_cg_params;
+
+typedef struct {
+  int converged;
+  int iterations;
+  double residual_norm;     /* recursive (plain) or FP64 true residual (mixed) */
+  double relative_residual; /* residual_norm / |b| (cg.jl:16-22)               */
+  int reason;               /* LMB_CG_*                                        */
+  int reliable_updates;
+  double true_residual_norm; /* |b - D'D x| in FP64 (mixed, and plain on exit) */
+  /* profile = 1: device time of the two stencil kernels of an iteration */
+  double dslash_ms, update_ms; /* K1 (tmp = D p, |tmp|^2) and K2 (D'tmp + axpy) */
+  int dslash_launches, update_launches;
+  long long kernel_launches; /* liblmb200 kernels launched by this solve    */
+} lmb_cg_result;
+
+/* ---- context --------------------------------------------------------------
+ * The context owns the repacked link / clover caches and the solver
+ * workspaces (WilsonDiracCloverOperator.jl:418-432 CloverCacheState;
+ * HISQFullSmearing.jl:340-354 HISQCacheState).  Field memory stays the
+ * caller's (CuArray or any device allocation). */
+lmb_ctx *lmb_create(int device);
+void lmb_destroy(lmb_ctx *ctx);
+const char *lmb_last_error(const lmb_ctx *ctx);
+int lmb_version(void);
+
+/* Lattice geometry of every field passed afterwards: local extents L (x
+ * fastest), halo width nw, fermion boundary phases (LatticeMatrix.phases,
+ * LatticeMatrices_core.jl:159-184; forward wrap * phase, backward wrap / phase,
+ * :707-723), Cartesian rank coordinates for the global staggered eta
+ * (LinearAlgebras/staggered.jl:43-57) and the element type of the fields
+ * (LMB_DTYPE_*).  Replaces the per-call ensure_halo!/set_halo! of a single
+ * rank (LatticeMatrices_core.jl:550-588) by in-kernel periodic indexing. */
+int lmb_set_geometry(lmb_ctx *ctx, const int L[4], int nw,
+                     const double phase_re[4], const double phase_im[4],
+                     const int coords[4], int dtype);
+
+/* Upload (repack) four link fields.  The cache is keyed by the pointers and
+ * the core epochs (halo_epoch.core), as _clover_cache_is_current
+ * (WilsonDiracCloverOperator.jl:603-625) and _ensure_hisq_cache_current!
+ * (HISQFullSmearing.jl:435-441): an unchanged (pointer, epoch) set is not
+ * re-read.  which = LMB_LINKS_*. */
+int lmb_links_upload(lmb_ctx *ctx, int which, const void *const U[4],
+                     const uint64_t epoch[4], void *stream);
+
+/* mul!(out, WilsonDiracOperator4D(U, kappa), in) and its adjoint
+ * (Operators/WilsonDiracOperator.jl:60-76, 420-438).  out != in. */
+int lmb_wilson_apply(lmb_ctx *ctx, void *out, const void *in, double kappa,
+                     int dagger, int precision, void *stream);
+
+/* mul!(out, WilsonDiracCloverOperator4D(U, kappa, cSW), in) / adjoint and
+ * mul_cached_clover! / mul_cached_clover_adjoint!
+ * (Operators/WilsonDiracCloverOperator.jl:561-601, 642-668).  The clover
+ * blocks are rebuilt when the links or kappa*cSW change (update_clover!,
+ * :392-399, 468-479). */
+int lmb_wilson_clover_apply(lmb_ctx *ctx, void *out, const void *in,
+                            double kappa, double csw, int dagger,
+                            int precision, void *stream);
+
+/* CloverFieldStrength4D(U) components (12,13,14,23,24,34) written to six
+ * padded (3,3,...) fields (Operators/WilsonDiracCloverOperator.jl:28-35,
+ * 392-399). */
+int lmb_clover_field_strength(lmb_ctx *ctx, void *const F[6], void *stream);
+
+/* cg!(x, DdagDOp(D, temp), b, r, p, Ap; rtol, atol, maxiter)
+ * (LinearAlgebras/cg.jl:73-137, Operators/DiracOperators.jl:93-143,
+ * benchmark/ddagd_cg/ddagd_cg.jl:587-644).  x holds the initial guess on entry
+ * and the solution on return; the work fields live in the context.
+ * Synchronises the stream. */
+int lmb_cg_ddagd(lmb_ctx *ctx, const lmb_cg_params *params, void *x,
+                 const void *b, lmb_cg_result *result, void *stream);
+
+/* dot(a, b) = sum conj(a) b over the core (LinearAlgebras/linearalgebra_D.jl:
+ * 3325-3341) of two padded fields with ncomp complex numbers per site.
+ * out[0] = Re, out[1] = Im.  Synchronises the stream. */
+int lmb_field_dot(lmb_ctx *ctx, const void *a, const void *b, int ncomp,
+                  double out[2], void *stream);
+
+
+/* Seeded synthetic inputs, decomposition independent (Philox4x32-10 site
+ * streams as utilities/randomgenerator.jl:247-340):
+ * U_mu(x) = reunitarize(exp(i amplitude H)) with H traceless Hermitian
+ * Gaussian (normalize_matrix!, LinearAlgebras/linearalgebra_D.jl:2340-2425),
+ * written to four padded (3,3,...) fields; and a unit-variance complex
+ * Gaussian field with ncomp numbers per site (randomize_gaussian_matrix!,
+ * linearalgebra_D.jl:2611-2652; re, im ~ N(0, 1/2) as
+ * benchmark/ddagd_cg/README.md:161-162). */
+int lmb_random_su3_links(lmb_ctx *ctx, void *const U[4], double amplitude,
+                         uint64_t seed, void *stream);
+int lmb_gaussian_field(lmb_ctx *ctx, void *out, int ncomp, uint64_t seed,
+                       void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LMB200_H */

@@ -1,0 +1,682 @@
+// lmb_capi.cu -- extern "C" entry points of liblmb200.so (declared in
+// include/lmb200.h) and the host drivers behind them.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "lmb_context.cuh"
+#include "lmb_random.cuh"
+
+using namespace lmb;
+
+namespace {
+
+cudaStream_t as_stream(void *s) { return (cudaStream_t)s; }
+
+bool ctx_ok(lmb_ctx *ctx) { return ctx != nullptr; }
+
+// ---------------------------------------------------------------------------
+// link caches
+// ---------------------------------------------------------------------------
+int ensure_link_precision(lmb_ctx *ctx, LinkSet &ls, int prec, cudaStream_t st) {
+  const int64_t n = 36 * ctx->g.V;
+  if (prec == PREC_SINGLE && ls.f_version != ls.version) {
+    if (!ls.f) LMB_CUDA(ctx, cudaMalloc(&ls.f, sizeof(float2) * n));
+    links_to_single_kernel<<<grid_for(n, 256), 256, 0, st>>>(ls.f, ls.d, n);
+    LMB_CHECK_LAUNCH(ctx);
+    ls.f_version = ls.version;
+  }
+  if (prec == PREC_HALF && ls.h_version != ls.version) {
+    if (!ls.h) LMB_CUDA(ctx, cudaMalloc(&ls.h, sizeof(int) * n));
+    links_to_half_kernel<<<grid_for(n, 256), 256, 0, st>>>(ls.h, ls.d, n, ls.scale);
+    LMB_CHECK_LAUNCH(ctx);
+    ls.h_version = ls.version;
+  }
+  return LMB_OK;
+}
+
+float device_absmax(lmb_ctx *ctx, const double2 *p, int64_t n, cudaStream_t st, int *rc) {
+  unsigned *bits = (unsigned *)workspace(ctx, "absmax", sizeof(unsigned));
+  if (!bits) { *rc = fail(ctx, LMB_ERR_CUDA, "out of device memory (absmax)"); return 1.f; }
+  cudaMemsetAsync(bits, 0, sizeof(unsigned), st);
+  absmax_kernel<<<1184, 256, 0, st>>>(p, n, bits);
+  unsigned h = 0;
+  cudaMemcpyAsync(&h, bits, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) { *rc = fail(ctx, LMB_ERR_CUDA, "absmax sync"); return 1.f; }
+  float f;
+  std::memcpy(&f, &h, sizeof f);
+  *rc = LMB_OK;
+  return f;
+}
+
+template <int P> Gauge<P> gauge_view(const LinkSet &ls, int64_t V);
+template <> Gauge<PREC_DOUBLE> gauge_view<PREC_DOUBLE>(const LinkSet &ls, int64_t V) { return {ls.d, V, ls.scale}; }
+template <> Gauge<PREC_SINGLE> gauge_view<PREC_SINGLE>(const LinkSet &ls, int64_t V) { return {ls.f, V, ls.scale}; }
+template <> Gauge<PREC_HALF> gauge_view<PREC_HALF>(const LinkSet &ls, int64_t V) { return {ls.h, V, ls.scale}; }
+
+// ---------------------------------------------------------------------------
+// clover cache
+// ---------------------------------------------------------------------------
+int ensure_field_strength(lmb_ctx *ctx, cudaStream_t st) {
+  CloverCache &cc = ctx->clover;
+  const LinkSet &ls = ctx->links[LMB_LINKS_THIN];
+  if (cc.F_valid && cc.F_links_version == ls.version) return LMB_OK;
+  const int64_t V = ctx->g.V;
+  if (!cc.F) LMB_CUDA(ctx, cudaMalloc(&cc.F, sizeof(double2) * 54 * V));
+  clover_field_strength_kernel<<<grid_for(6 * V, 128), 128, 0, st>>>(cc.F, ls.d, ctx->g);
+  LMB_CHECK_LAUNCH(ctx);
+  cc.F_valid = true;
+  cc.F_links_version = ls.version;
+  return LMB_OK;
+}
+
+int ensure_clover(lmb_ctx *ctx, double coef, int prec, cudaStream_t st) {
+  CloverCache &cc = ctx->clover;
+  const LinkSet &ls = ctx->links[LMB_LINKS_THIN];
+  const int64_t V = ctx->g.V;
+  int rc = ensure_field_strength(ctx, st);
+  if (rc) return rc;
+  if (!cc.d_valid || cc.links_version != ls.version || cc.coef != coef) {
+    if (!cc.d) LMB_CUDA(ctx, cudaMalloc(&cc.d, sizeof(double2) * 36 * V));
+    clover_blocks_double_kernel<<<grid_for(V, 128), 128, 0, st>>>(cc.d, cc.F, ctx->g, coef);
+    LMB_CHECK_LAUNCH(ctx);
+    cc.d_valid = true;
+    cc.links_version = ls.version;
+    cc.coef = coef;
+    cc.d_version++;
+  }
+  if (prec == PREC_SINGLE && cc.f_version != cc.d_version) {
+    if (!cc.f) LMB_CUDA(ctx, cudaMalloc(&cc.f, sizeof(float4) * 18 * V));
+    clover_to_single_kernel<<<grid_for(V, 256), 256, 0, st>>>(cc.f, cc.d, V);
+    LMB_CHECK_LAUNCH(ctx);
+    cc.f_version = cc.d_version;
+  }
+  if (prec == PREC_HALF && cc.h_version != cc.d_version) {
+    if (!cc.h) LMB_CUDA(ctx, cudaMalloc(&cc.h, sizeof(int4) * 8 * V));
+    if (!cc.ht) LMB_CUDA(ctx, cudaMalloc(&cc.ht, sizeof(int2) * 2 * V));
+    cc.scale = device_absmax(ctx, cc.d, 36 * V, st, &rc);
+    if (rc) return rc;
+    clover_to_half_kernel<<<grid_for(V, 256), 256, 0, st>>>(cc.h, cc.ht, cc.d, V, cc.scale);
+    LMB_CHECK_LAUNCH(ctx);
+    cc.h_version = cc.d_version;
+  }
+  return LMB_OK;
+}
+
+template <int P> Clover<P> clover_view(const CloverCache &cc, int64_t V);
+template <> Clover<PREC_DOUBLE> clover_view<PREC_DOUBLE>(const CloverCache &cc, int64_t V) { return {cc.d, V, cc.scale}; }
+template <> Clover<PREC_SINGLE> clover_view<PREC_SINGLE>(const CloverCache &cc, int64_t V) { return {cc.f, V, cc.scale}; }
+template <> Clover<PREC_HALF> clover_view<PREC_HALF>(const CloverCache &cc, int64_t V) {
+  Clover<PREC_HALF> c;
+  c.data = cc.h;
+  c.tail = cc.ht;
+  c.V = V;
+  c.scale = cc.scale;
+  return c;
+}
+
+// ---------------------------------------------------------------------------
+// stencil launch
+// ---------------------------------------------------------------------------
+template <int PS, int PG, bool CLOVER, class Epi>
+int launch_wilson(lmb_ctx *ctx, const Field<PS, 12> &in, int dagger, double kappa, const Epi &epi,
+                  cudaStream_t st) {
+  typedef typename Real<PS>::type R;
+  const Geom &g = ctx->g;
+  const Gauge<PG> U = gauge_view<PG>(ctx->links[LMB_LINKS_THIN], g.V);
+  const unsigned grid = grid_for(g.V, kDslashThreads);
+  if constexpr (CLOVER) {
+    const Clover<PG> A = clover_view<PG>(ctx->clover, g.V);
+    if (dagger)
+      wilson_dslash_kernel<R, 1, true><<<grid, kDslashThreads, 0, st>>>(g, in, U, A, (R)kappa, epi);
+    else
+      wilson_dslash_kernel<R, 0, true><<<grid, kDslashThreads, 0, st>>>(g, in, U, A, (R)kappa, epi);
+  } else {
+    const NoClover A{g.V};
+    if (dagger)
+      wilson_dslash_kernel<R, 1, false><<<grid, kDslashThreads, 0, st>>>(g, in, U, A, (R)kappa, epi);
+    else
+      wilson_dslash_kernel<R, 0, false><<<grid, kDslashThreads, 0, st>>>(g, in, U, A, (R)kappa, epi);
+  }
+  LMB_CHECK_LAUNCH(ctx);
+  return LMB_OK;
+}
+
+template <int PS, class Epi>
+int launch_op(lmb_ctx *ctx, int op, const Field<PS, 12> &in, int dagger, double kappa, const Epi &epi,
+              cudaStream_t st) {
+  if (op == LMB_OP_WILSON_CLOVER) return launch_wilson<PS, PS, true>(ctx, in, dagger, kappa, epi, st);
+  return launch_wilson<PS, PS, false>(ctx, in, dagger, kappa, epi, st);
+}
+
+int prepare_operator(lmb_ctx *ctx, int op, double kappa, double csw, int prec, cudaStream_t st) {
+  if (!ctx->geom_set) return fail(ctx, LMB_ERR_STATE, "lmb_set_geometry has not been called");
+  if (op != LMB_OP_WILSON && op != LMB_OP_WILSON_CLOVER)
+    return fail(ctx, LMB_ERR_UNSUPPORTED, "operator %d is not available in this build", op);
+  if (!ctx->links[LMB_LINKS_THIN].valid) return fail(ctx, LMB_ERR_STATE, "gauge links have not been uploaded");
+  if (prec < PREC_DOUBLE || prec > PREC_HALF) return fail(ctx, LMB_ERR_ARG, "unknown precision %d", prec);
+  int rc = ensure_link_precision(ctx, ctx->links[LMB_LINKS_THIN], prec, st);
+  if (rc) return rc;
+  if (op == LMB_OP_WILSON_CLOVER) return ensure_clover(ctx, -kappa * csw, prec, st);
+  return LMB_OK;
+}
+
+template <int PS, int NC>
+int pack_in(lmb_ctx *ctx, Field<PS, NC> &f, const void *src, cudaStream_t st) {
+  const unsigned grid = grid_for(ctx->g.V, 256);
+  if (ctx->dtype == LMB_DTYPE_C128)
+    pack_field_kernel<double2, PS, NC><<<grid, 256, 0, st>>>(f, (const double2 *)src, ctx->g, ctx->pd);
+  else
+    pack_field_kernel<float2, PS, NC><<<grid, 256, 0, st>>>(f, (const float2 *)src, ctx->g, ctx->pd);
+  LMB_CHECK_LAUNCH(ctx);
+  return LMB_OK;
+}
+
+template <int PS, int NC>
+int unpack_out(lmb_ctx *ctx, void *dst, const Field<PS, NC> &f, cudaStream_t st) {
+  const unsigned grid = grid_for(ctx->g.V, 256);
+  if (ctx->dtype == LMB_DTYPE_C128)
+    unpack_field_kernel<double2, PS, NC><<<grid, 256, 0, st>>>((double2 *)dst, f, ctx->g, ctx->pd);
+  else
+    unpack_field_kernel<float2, PS, NC><<<grid, 256, 0, st>>>((float2 *)dst, f, ctx->g, ctx->pd);
+  LMB_CHECK_LAUNCH(ctx);
+  return LMB_OK;
+}
+
+template <int PS>
+int apply_wilson_family(lmb_ctx *ctx, int op, void *out, const void *in, double kappa, int dagger,
+                        cudaStream_t st) {
+  Field<PS, 12> fin, fout;
+  if (!make_field(ctx, "apply_in", fin) || !make_field(ctx, "apply_out", fout))
+    return fail(ctx, LMB_ERR_CUDA, "out of device memory (apply workspaces)");
+  int rc = pack_in(ctx, fin, in, st);
+  if (rc) return rc;
+  EpiStore<PS> epi{fout, nullptr};
+  rc = launch_op<PS>(ctx, op, fin, dagger, kappa, epi, st);
+  if (rc) return rc;
+  return unpack_out(ctx, out, fout, st);
+}
+
+int apply_dispatch(lmb_ctx *ctx, int op, void *out, const void *in, double kappa, double csw, int dagger,
+                   int prec, void *stream) {
+  if (!ctx_ok(ctx)) return LMB_ERR_ARG;
+  if (!out || !in) return fail(ctx, LMB_ERR_ARG, "null field pointer");
+  if (out == in) return fail(ctx, LMB_ERR_ARG, "mul! requires distinct result and input fields");
+  cudaStream_t st = as_stream(stream);
+  int rc = prepare_operator(ctx, op, kappa, csw, prec, st);
+  if (rc) return rc;
+  switch (prec) {
+    case PREC_DOUBLE: return apply_wilson_family<PREC_DOUBLE>(ctx, op, out, in, kappa, dagger, st);
+    case PREC_SINGLE: return apply_wilson_family<PREC_SINGLE>(ctx, op, out, in, kappa, dagger, st);
+    default: return apply_wilson_family<PREC_HALF>(ctx, op, out, in, kappa, dagger, st);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// CG driver
+// ---------------------------------------------------------------------------
+struct EventPool {
+  std::vector<cudaEvent_t> ev;
+  void ensure(size_t n) {
+    while (ev.size() < n) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      ev.push_back(e);
+    }
+  }
+  ~EventPool() {
+    for (auto e : ev) cudaEventDestroy(e);
+  }
+};
+
+int read_state(lmb_ctx *ctx, cudaStream_t st) {
+  LMB_CUDA(ctx, cudaMemcpyAsync(ctx->st_host, ctx->st_dev, sizeof(CGState), cudaMemcpyDeviceToHost, st));
+  LMB_CUDA(ctx, cudaStreamSynchronize(st));
+  return LMB_OK;
+}
+
+// PS: precision of the iterated fields (DOUBLE = plain FP64 CG), PX: of x_low
+template <int PS, int PX>
+int cg_run(lmb_ctx *ctx, const lmb_cg_params *prm, void *x_pad, const void *b_pad, lmb_cg_result *res,
+           cudaStream_t st) {
+  constexpr bool mixed = PS != PREC_DOUBLE;
+  const int64_t V = ctx->g.V;
+  const int op = prm->op;
+  const double kappa = prm->kappa;
+  int rc;
+  long long nl = 0;  // liblmb200 kernels launched by this solve
+  Field<PREC_DOUBLE, 12> b64, x64, r64, t64;
+  if (!make_field(ctx, "cg_b", b64) || !make_field(ctx, "cg_x", x64) || !make_field(ctx, "cg_r", r64) ||
+      !make_field(ctx, "cg_t", t64))
+    return fail(ctx, LMB_ERR_CUDA, "out of device memory (CG FP64 fields)");
+  Field<PS, 12> p, rl, tl;
+  Field<PX, 12> xl;
+  if (!make_field(ctx, "cg_p", p)) return fail(ctx, LMB_ERR_CUDA, "out of device memory (CG p)");
+  if constexpr (mixed) {
+    if (!make_field(ctx, "cg_rl", rl) || !make_field(ctx, "cg_tl", tl) || !make_field(ctx, "cg_xl", xl))
+      return fail(ctx, LMB_ERR_CUDA, "out of device memory (CG low-precision fields)");
+  } else {
+    rl = *(Field<PS, 12> *)&r64;
+    tl = *(Field<PS, 12> *)&t64;
+    xl = *(Field<PX, 12> *)&x64;
+  }
+  const unsigned dgrid = grid_for(V, kDslashThreads), bgrid = grid_for(V, kBlasThreads);
+  if (!ensure_partials(ctx, dgrid > bgrid ? dgrid : bgrid, 1))
+    return fail(ctx, LMB_ERR_CUDA, "out of device memory (reduction partials)");
+  rc = prepare_operator(ctx, op, kappa, prm->csw, PREC_DOUBLE, st);
+  if (rc) return rc;
+  if (mixed) {
+    rc = prepare_operator(ctx, op, kappa, prm->csw, PS, st);
+    if (rc) return rc;
+  }
+
+  // initial state
+  CGState init{};
+  init.delta2 = mixed ? prm->delta * prm->delta : 0.0;
+  init.maxiter = prm->maxiter;
+  init.status = ST_RUNNING;
+  LMB_CUDA(ctx, cudaMemcpyAsync(ctx->st_dev, &init, sizeof init, cudaMemcpyHostToDevice, st));
+  rc = pack_in(ctx, b64, b_pad, st);
+  if (rc) return rc;
+  rc = pack_in(ctx, x64, x_pad, st);
+  if (rc) return rc;
+  nl += 2;
+  if constexpr (mixed) {
+    LMB_CUDA(ctx, cudaMemsetAsync(xl.data, 0, Field<PX, 12>::bytes(V), st));
+    if (xl.norm) LMB_CUDA(ctx, cudaMemsetAsync(xl.norm, 0, Field<PX, 12>::norm_bytes(V), st));
+  }
+  norm_b_kernel<12><<<bgrid, kBlasThreads, 0, st>>>(b64, ctx->st_dev, V, prm->rtol, prm->atol, ctx->partials,
+                                                     ctx->counter);
+  LMB_CHECK_LAUNCH(ctx);
+  nl++;
+  // r = b - D'D x (FP64)
+  auto true_residual = [&](int mode) -> int {
+    EpiStore<PREC_DOUBLE> e1{t64, nullptr};
+    int r2 = launch_op<PREC_DOUBLE>(ctx, op, x64, 0, kappa, e1, st);
+    if (r2) return r2;
+    nl += 2;
+    EpiTrueResidual<PS> e2{b64, r64, rl, mixed ? 1 : 0, mode, ctx->st_dev, ctx->partials, ctx->counter};
+    return launch_op<PREC_DOUBLE>(ctx, op, t64, 1, kappa, e2, st);
+  };
+  rc = true_residual(0);
+  if (rc) return rc;
+  convert_kernel<PS, PS, 12><<<bgrid, kBlasThreads, 0, st>>>(p, rl, V);
+  LMB_CHECK_LAUNCH(ctx);
+  nl++;
+  rc = read_state(ctx, st);
+  if (rc) return rc;
+  CGState *hs = ctx->st_host;
+  if (!std::isfinite(hs->bb)) hs->status = ST_BREAKDOWN;
+  if (hs->status == ST_RUNNING && prm->maxiter == 0) hs->status = ST_MAXITER;
+  if (hs->status != ST_RUNNING)
+    LMB_CUDA(ctx, cudaMemcpyAsync(ctx->st_dev, hs, sizeof(CGState), cudaMemcpyHostToDevice, st));
+
+  const int k = prm->check_interval > 0 ? prm->check_interval : 8;
+  EventPool pool;
+  if (prm->profile) pool.ensure(4 * (size_t)k);
+  double k1_ms = 0, k2_ms = 0;
+  int k1_n = 0, k2_n = 0;
+
+  EpiStoreNorm<PS> epi1{tl, ctx->st_dev, ctx->partials, ctx->counter};
+  EpiCGUpdate<PS, PX> epi2{p, rl, xl, ctx->st_dev, ctx->partials, ctx->counter};
+  while (hs->status == ST_RUNNING) {
+    const int it0 = hs->iter;
+    for (int i = 0; i < k; i++) {
+      if (prm->profile) cudaEventRecord(pool.ev[4 * i], st);
+      rc = launch_op<PS>(ctx, op, p, 0, kappa, epi1, st);
+      if (rc) return rc;
+      nl++;
+      if (prm->profile) cudaEventRecord(pool.ev[4 * i + 1], st);
+      rc = launch_op<PS>(ctx, op, tl, 1, kappa, epi2, st);
+      if (rc) return rc;
+      nl++;
+      if (prm->profile) cudaEventRecord(pool.ev[4 * i + 2], st);
+      cg_p_update_kernel<PS, 12><<<bgrid, kBlasThreads, 0, st>>>(p, rl, ctx->st_dev, V);
+      LMB_CHECK_LAUNCH(ctx);
+  nl++;
+      if (prm->profile) cudaEventRecord(pool.ev[4 * i + 3], st);
+    }
+    rc = read_state(ctx, st);
+    if (rc) return rc;
+    if (prm->profile) {
+      const int real = hs->iter - it0 + (hs->status == ST_RELIABLE ? 1 : 0);
+      for (int i = 0; i < real && i < k; i++) {
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, pool.ev[4 * i], pool.ev[4 * i + 1]);
+        cudaEventElapsedTime(&b, pool.ev[4 * i + 1], pool.ev[4 * i + 2]);
+        k1_ms += a;
+        k2_ms += b;
+        k1_n++;
+        k2_n++;
+      }
+    }
+    if (hs->status == ST_RELIABLE) {
+      if constexpr (mixed) {
+        fold_kernel<PX, 12><<<bgrid, kBlasThreads, 0, st>>>(x64, xl, V);
+        LMB_CHECK_LAUNCH(ctx);
+  nl++;
+        // resume: the true-residual kernel runs regardless of the pause
+        rc = true_residual(1);
+        if (rc) return rc;
+        cg_p_update_kernel<PS, 12><<<bgrid, kBlasThreads, 0, st>>>(p, rl, ctx->st_dev, V);
+        LMB_CHECK_LAUNCH(ctx);
+  nl++;
+        rc = read_state(ctx, st);
+        if (rc) return rc;
+      }
+    }
+  }
+  if constexpr (mixed) {
+    fold_kernel<PX, 12><<<bgrid, kBlasThreads, 0, st>>>(x64, xl, V);
+    LMB_CHECK_LAUNCH(ctx);
+  nl++;
+  }
+  const int status = hs->status;
+  CGState final_state = *hs;
+  // true residual for the report (does not change the outcome)
+  if (!mixed || status != ST_CONVERGED) {
+    rc = true_residual(2);
+    if (rc) return rc;
+    rc = read_state(ctx, st);
+    if (rc) return rc;
+  }
+  const double rr_true = ctx->st_host->rr_true;
+  rc = unpack_out(ctx, x_pad, x64, st);
+  if (rc) return rc;
+  nl++;
+  LMB_CUDA(ctx, cudaStreamSynchronize(st));
+
+  const double bn = std::sqrt(final_state.bb);
+  double rn;
+  if (status == ST_BREAKDOWN) rn = NAN;
+  else rn = mixed ? std::sqrt(final_state.rr_true) : std::sqrt(final_state.rr);
+  if (mixed && status != ST_CONVERGED && status != ST_BREAKDOWN) rn = std::sqrt(rr_true);
+  res->converged = status == ST_CONVERGED;
+  res->iterations = final_state.iter;
+  res->residual_norm = rn;
+  res->relative_residual = bn == 0.0 ? (rn == 0.0 ? 0.0 : INFINITY) : rn / bn;
+  switch (status) {
+    case ST_CONVERGED: res->reason = LMB_CG_CONVERGED; break;
+    case ST_MAXITER: res->reason = LMB_CG_MAXIMUM_ITERATIONS; break;
+    case ST_NONPOSITIVE: res->reason = LMB_CG_NONPOSITIVE_CURVATURE; break;
+    default: res->reason = LMB_CG_NUMERICAL_BREAKDOWN; break;
+  }
+  res->reliable_updates = final_state.reliable_updates;
+  res->true_residual_norm = std::sqrt(rr_true);
+  res->dslash_ms = k1_ms;
+  res->update_ms = k2_ms;
+  res->dslash_launches = k1_n;
+  res->update_launches = k2_n;
+  res->kernel_launches = nl;
+  return LMB_OK;
+}
+
+template <int NC>
+__global__ void __launch_bounds__(256)
+    dot_kernel(const void *a, const void *b, int c64, Geom g, Padded pd, double *partials, unsigned *counter,
+               double *out) {
+  const int s = blockIdx.x * 256 + threadIdx.x;
+  double v[2] = {0.0, 0.0}, tot[2];
+  if (s < g.V) {
+    int c[4];
+    site_coords(g, s, c);
+    const int64_t off = padded_site(pd, c) * NC;
+    for (int k = 0; k < NC; k++) {
+      double ar, ai, br, bi;
+      if (c64) {
+        const float2 x = ((const float2 *)a)[off + k], y = ((const float2 *)b)[off + k];
+        ar = x.x; ai = x.y; br = y.x; bi = y.y;
+      } else {
+        const double2 x = ((const double2 *)a)[off + k], y = ((const double2 *)b)[off + k];
+        ar = x.x; ai = x.y; br = y.x; bi = y.y;
+      }
+      v[0] += ar * br + ai * bi;
+      v[1] += ar * bi - ai * br;
+    }
+  }
+  if (grid_reduce<256, 2>(v, partials, counter, tot) && threadIdx.x == 0) {
+    out[0] = tot[0];
+    out[1] = tot[1];
+  }
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int lmb_version(void) { return 100; }
+
+lmb_ctx *lmb_create(int device) {
+  if (cudaSetDevice(device) != cudaSuccess) return nullptr;
+  lmb_ctx *ctx = new lmb_ctx();
+  ctx->device = device;
+  if (cudaMalloc(&ctx->counter, sizeof(unsigned)) != cudaSuccess ||
+      cudaMemset(ctx->counter, 0, sizeof(unsigned)) != cudaSuccess ||
+      cudaMalloc(&ctx->st_dev, sizeof(CGState)) != cudaSuccess ||
+      cudaMallocHost(&ctx->st_host, sizeof(CGState)) != cudaSuccess ||
+      cudaMallocHost(&ctx->dot_host, 2 * sizeof(double)) != cudaSuccess) {
+    lmb_destroy(ctx);
+    return nullptr;
+  }
+  return ctx;
+}
+
+void lmb_destroy(lmb_ctx *ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  for (auto &kv : ctx->buffers) cudaFree(kv.second.first);
+  for (auto &ls : ctx->links) {
+    cudaFree(ls.d);
+    cudaFree(ls.f);
+    cudaFree(ls.h);
+  }
+  cudaFree(ctx->clover.F);
+  cudaFree(ctx->clover.d);
+  cudaFree(ctx->clover.f);
+  cudaFree(ctx->clover.h);
+  cudaFree(ctx->clover.ht);
+  cudaFree(ctx->partials);
+  cudaFree(ctx->counter);
+  cudaFree(ctx->st_dev);
+  if (ctx->st_host) cudaFreeHost(ctx->st_host);
+  if (ctx->dot_host) cudaFreeHost(ctx->dot_host);
+  delete ctx;
+}
+
+const char *lmb_last_error(const lmb_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int lmb_set_geometry(lmb_ctx *ctx, const int L[4], int nw, const double phase_re[4], const double phase_im[4],
+                     const int coords[4], int dtype) {
+  if (!ctx_ok(ctx)) return LMB_ERR_ARG;
+  if (!L || !phase_re || !phase_im) return fail(ctx, LMB_ERR_ARG, "null geometry argument");
+  if (nw < 0) return fail(ctx, LMB_ERR_ARG, "nw must be non-negative, got %d", nw);
+  if (dtype != LMB_DTYPE_C128 && dtype != LMB_DTYPE_C64) return fail(ctx, LMB_ERR_ARG, "unknown dtype %d", dtype);
+  int64_t V = 1;
+  for (int mu = 0; mu < 4; mu++) {
+    if (L[mu] <= 0) return fail(ctx, LMB_ERR_ARG, "global lattice sizes must be positive, got %d", L[mu]);
+    if (nw > L[mu])
+      return fail(ctx, LMB_ERR_ARG, "halo width nw=%d exceeds local lattice size %d in dimension %d", nw, L[mu],
+                  mu + 1);
+    const double re = phase_re[mu], im = phase_im[mu];
+    if (re == 0.0 && im == 0.0)
+      return fail(ctx, LMB_ERR_ARG, "boundary phases must be nonzero because negative wraps use inv(phase)");
+    V *= L[mu];
+  }
+  if (V > (int64_t)0x7fffffff / 4) return fail(ctx, LMB_ERR_ARG, "local volume too large for one GPU context");
+  Geom g{};
+  int stride = 1;
+  for (int mu = 0; mu < 4; mu++) {
+    g.L[mu] = L[mu];
+    g.stride[mu] = stride;
+    stride *= L[mu];
+    const double re = phase_re[mu], im = phase_im[mu], n = re * re + im * im;
+    g.ph_fwd[mu][0] = re;
+    g.ph_fwd[mu][1] = im;
+    g.ph_bwd[mu][0] = re / n;
+    g.ph_bwd[mu][1] = -im / n;
+    if (!(re == 1.0 && im == 0.0)) g.phase_mask |= 1 << mu;
+    g.eta_off[mu] = coords ? coords[mu] * L[mu] : 0;
+  }
+  g.V = V;
+  const bool changed = !ctx->geom_set || std::memcmp(&g, &ctx->g, sizeof g) != 0 || ctx->pd.nw != nw ||
+                       ctx->dtype != dtype;
+  ctx->g = g;
+  ctx->pd.nw = nw;
+  for (int mu = 0; mu < 4; mu++) ctx->pd.P[mu] = L[mu] + 2 * nw;
+  ctx->dtype = dtype;
+  ctx->geom_set = true;
+  if (changed)
+    for (auto &ls : ctx->links) ls.valid = false;
+  return LMB_OK;
+}
+
+int lmb_links_upload(lmb_ctx *ctx, int which, const void *const U[4], const uint64_t epoch[4], void *stream) {
+  if (!ctx_ok(ctx)) return LMB_ERR_ARG;
+  if (!ctx->geom_set) return fail(ctx, LMB_ERR_STATE, "lmb_set_geometry has not been called");
+  if (which < 0 || which > 2) return fail(ctx, LMB_ERR_ARG, "unknown link set %d", which);
+  if (!U) return fail(ctx, LMB_ERR_ARG, "null link array");
+  for (int mu = 0; mu < 4; mu++)
+    if (!U[mu]) return fail(ctx, LMB_ERR_ARG, "gauge link U[%d] is null", mu + 1);
+  LinkSet &ls = ctx->links[which];
+  bool same = ls.valid;
+  for (int mu = 0; mu < 4 && same; mu++)
+    same = ls.ptr[mu] == U[mu] && epoch && ls.epoch[mu] == epoch[mu];
+  if (same) return LMB_OK;
+  cudaStream_t st = as_stream(stream);
+  const int64_t V = ctx->g.V;
+  if (!ls.d) LMB_CUDA(ctx, cudaMalloc(&ls.d, sizeof(double2) * 36 * V));
+  if (ctx->dtype == LMB_DTYPE_C128)
+    pack_links_kernel<double2><<<grid_for(V, 256), 256, 0, st>>>(
+        ls.d, (const double2 *)U[0], (const double2 *)U[1], (const double2 *)U[2], (const double2 *)U[3], ctx->g,
+        ctx->pd);
+  else
+    pack_links_kernel<float2><<<grid_for(V, 256), 256, 0, st>>>(ls.d, (const float2 *)U[0], (const float2 *)U[1],
+                                                                (const float2 *)U[2], (const float2 *)U[3],
+                                                                ctx->g, ctx->pd);
+  LMB_CHECK_LAUNCH(ctx);
+  int rc;
+  ls.scale = device_absmax(ctx, ls.d, 36 * V, st, &rc);
+  if (rc) return rc;
+  for (int mu = 0; mu < 4; mu++) {
+    ls.ptr[mu] = U[mu];
+    ls.epoch[mu] = epoch ? epoch[mu] : 0;
+  }
+  ls.valid = true;
+  ls.version++;
+  return LMB_OK;
+}
+
+int lmb_wilson_apply(lmb_ctx *ctx, void *out, const void *in, double kappa, int dagger, int precision,
+                     void *stream) {
+  return apply_dispatch(ctx, LMB_OP_WILSON, out, in, kappa, 0.0, dagger, precision, stream);
+}
+
+int lmb_wilson_clover_apply(lmb_ctx *ctx, void *out, const void *in, double kappa, double csw, int dagger,
+                            int precision, void *stream) {
+  return apply_dispatch(ctx, LMB_OP_WILSON_CLOVER, out, in, kappa, csw, dagger, precision, stream);
+}
+
+int lmb_clover_field_strength(lmb_ctx *ctx, void *const F[6], void *stream) {
+  if (!ctx_ok(ctx)) return LMB_ERR_ARG;
+  if (!ctx->geom_set) return fail(ctx, LMB_ERR_STATE, "lmb_set_geometry has not been called");
+  if (!ctx->links[LMB_LINKS_THIN].valid) return fail(ctx, LMB_ERR_STATE, "gauge links have not been uploaded");
+  cudaStream_t st = as_stream(stream);
+  int rc = ensure_field_strength(ctx, st);
+  if (rc) return rc;
+  for (int p = 0; p < 6; p++) {
+    if (!F[p]) return fail(ctx, LMB_ERR_ARG, "null field-strength pointer %d", p);
+    Field<PREC_DOUBLE, 9> f;
+    f.data = ctx->clover.F + (size_t)p * 9 * ctx->g.V;
+    f.norm = nullptr;
+    f.V = ctx->g.V;
+    rc = unpack_out(ctx, F[p], f, st);
+    if (rc) return rc;
+  }
+  return LMB_OK;
+}
+
+int lmb_cg_ddagd(lmb_ctx *ctx, const lmb_cg_params *prm, void *x, const void *b, lmb_cg_result *res,
+                 void *stream) {
+  if (!ctx_ok(ctx)) return LMB_ERR_ARG;
+  if (!prm || !res || !x || !b) return fail(ctx, LMB_ERR_ARG, "null argument");
+  if (x == b) return fail(ctx, LMB_ERR_ARG, "CG fields x and b must not alias");
+  if (!(prm->rtol >= 0)) return fail(ctx, LMB_ERR_ARG, "rtol must be nonnegative");
+  if (!(prm->atol >= 0)) return fail(ctx, LMB_ERR_ARG, "atol must be nonnegative");
+  if (!std::isfinite(prm->rtol)) return fail(ctx, LMB_ERR_ARG, "rtol must be finite");
+  if (!std::isfinite(prm->atol)) return fail(ctx, LMB_ERR_ARG, "atol must be finite");
+  if (prm->maxiter < 0) return fail(ctx, LMB_ERR_ARG, "maxiter must be nonnegative");
+  if (prm->precision != PREC_DOUBLE && !(prm->delta > 0 && prm->delta < 1))
+    return fail(ctx, LMB_ERR_ARG, "reliable-update delta must lie in (0, 1)");
+  std::memset(res, 0, sizeof *res);
+  cudaStream_t st = as_stream(stream);
+  switch (prm->precision) {
+    case PREC_DOUBLE: return cg_run<PREC_DOUBLE, PREC_DOUBLE>(ctx, prm, x, b, res, st);
+    case PREC_SINGLE: return cg_run<PREC_SINGLE, PREC_SINGLE>(ctx, prm, x, b, res, st);
+    case PREC_HALF: return cg_run<PREC_HALF, PREC_SINGLE>(ctx, prm, x, b, res, st);
+    default: return fail(ctx, LMB_ERR_ARG, "unknown precision %d", prm->precision);
+  }
+}
+
+int lmb_field_dot(lmb_ctx *ctx, const void *a, const void *b, int ncomp, double out[2], void *stream) {
+  if (!ctx_ok(ctx)) return LMB_ERR_ARG;
+  if (!ctx->geom_set) return fail(ctx, LMB_ERR_STATE, "lmb_set_geometry has not been called");
+  if (!a || !b || !out) return fail(ctx, LMB_ERR_ARG, "null argument");
+  cudaStream_t st = as_stream(stream);
+  const unsigned grid = grid_for(ctx->g.V, 256);
+  if (!ensure_partials(ctx, grid, 2)) return fail(ctx, LMB_ERR_CUDA, "out of device memory (partials)");
+  double *dout = (double *)workspace(ctx, "dot_out", 2 * sizeof(double));
+  if (!dout) return fail(ctx, LMB_ERR_CUDA, "out of device memory (dot)");
+  const int c64 = ctx->dtype == LMB_DTYPE_C64;
+  switch (ncomp) {
+    case 1: dot_kernel<1><<<grid, 256, 0, st>>>(a, b, c64, ctx->g, ctx->pd, ctx->partials, ctx->counter, dout); break;
+    case 3: dot_kernel<3><<<grid, 256, 0, st>>>(a, b, c64, ctx->g, ctx->pd, ctx->partials, ctx->counter, dout); break;
+    case 9: dot_kernel<9><<<grid, 256, 0, st>>>(a, b, c64, ctx->g, ctx->pd, ctx->partials, ctx->counter, dout); break;
+    case 12: dot_kernel<12><<<grid, 256, 0, st>>>(a, b, c64, ctx->g, ctx->pd, ctx->partials, ctx->counter, dout); break;
+    default: return fail(ctx, LMB_ERR_UNSUPPORTED, "dot over %d components per site is not provided", ncomp);
+  }
+  LMB_CHECK_LAUNCH(ctx);
+  LMB_CUDA(ctx, cudaMemcpyAsync(ctx->dot_host, dout, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  LMB_CUDA(ctx, cudaStreamSynchronize(st));
+  out[0] = ctx->dot_host[0];
+  out[1] = ctx->dot_host[1];
+  return LMB_OK;
+}
+
+
+int lmb_random_su3_links(lmb_ctx *ctx, void *const U[4], double amplitude, uint64_t seed, void *stream) {
+  if (!ctx_ok(ctx)) return LMB_ERR_ARG;
+  if (!ctx->geom_set) return fail(ctx, LMB_ERR_STATE, "lmb_set_geometry has not been called");
+  if (!U) return fail(ctx, LMB_ERR_ARG, "null link array");
+  for (int mu = 0; mu < 4; mu++)
+    if (!U[mu]) return fail(ctx, LMB_ERR_ARG, "gauge link U[%d] is null", mu + 1);
+  cudaStream_t st = as_stream(stream);
+  const unsigned grid = grid_for(4 * ctx->g.V, 128);
+  if (ctx->dtype == LMB_DTYPE_C128)
+    random_su3_kernel<double2><<<grid, 128, 0, st>>>((double2 *)U[0], (double2 *)U[1], (double2 *)U[2],
+                                                      (double2 *)U[3], ctx->g, ctx->pd, amplitude, seed);
+  else
+    random_su3_kernel<float2><<<grid, 128, 0, st>>>((float2 *)U[0], (float2 *)U[1], (float2 *)U[2],
+                                                     (float2 *)U[3], ctx->g, ctx->pd, amplitude, seed);
+  LMB_CHECK_LAUNCH(ctx);
+  return LMB_OK;
+}
+
+int lmb_gaussian_field(lmb_ctx *ctx, void *out, int ncomp, uint64_t seed, void *stream) {
+  if (!ctx_ok(ctx)) return LMB_ERR_ARG;
+  if (!ctx->geom_set) return fail(ctx, LMB_ERR_STATE, "lmb_set_geometry has not been called");
+  if (!out) return fail(ctx, LMB_ERR_ARG, "null field");
+  if (ncomp <= 0) return fail(ctx, LMB_ERR_ARG, "ncomp must be positive");
+  cudaStream_t st = as_stream(stream);
+  const unsigned grid = grid_for(ctx->g.V, 256);
+  if (ctx->dtype == LMB_DTYPE_C128)
+    gaussian_field_kernel<double2><<<grid, 256, 0, st>>>((double2 *)out, ncomp, ctx->g, ctx->pd, seed);
+  else
+    gaussian_field_kernel<float2><<<grid, 256, 0, st>>>((float2 *)out, ncomp, ctx->g, ctx->pd, seed);
+  LMB_CHECK_LAUNCH(ctx);
+  return LMB_OK;
+}
+
+}  // extern "C"

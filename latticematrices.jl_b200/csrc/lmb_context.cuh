@@ -1,0 +1,131 @@
+// lmb_context.cuh -- the lmb_ctx object behind the C ABI: geometry, link and
+// clover caches, named workspaces and error reporting.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <map>
+#include <string>
+
+#include "../../include/lmb200.h"
+#include "lmb_pack.cuh"
+#include "lmb_solver.cuh"
+
+namespace lmb {
+
+struct LinkSet {
+  const void *ptr[4] = {nullptr, nullptr, nullptr, nullptr};
+  uint64_t epoch[4] = {0, 0, 0, 0};
+  bool valid = false;
+  uint64_t version = 0;  // bumps on every repack
+  double2 *d = nullptr;  // 36 planes
+  float2 *f = nullptr;
+  int *h = nullptr;
+  float scale = 1.f;     // max |element| (for int16)
+  uint64_t f_version = ~0ull, h_version = ~0ull;
+};
+
+struct CloverCache {
+  uint64_t links_version = ~0ull;
+  double coef = 0.0;
+  bool F_valid = false;
+  uint64_t F_links_version = ~0ull;
+  double2 *F = nullptr;  // 54 planes
+  double2 *d = nullptr;  // 36 planes
+  float4 *f = nullptr;
+  int4 *h = nullptr;
+  int2 *ht = nullptr;
+  float scale = 1.f;
+  bool d_valid = false;
+  uint64_t f_version = ~0ull, h_version = ~0ull, d_version = 0;
+};
+
+}  // namespace lmb
+
+struct lmb_ctx {
+  int device = 0;
+  bool geom_set = false;
+  lmb::Geom g{};
+  lmb::Padded pd{};
+  int dtype = LMB_DTYPE_C128;
+  lmb::LinkSet links[3];
+  lmb::CloverCache clover;
+  std::map<std::string, std::pair<void *, size_t>> buffers;
+  double *partials = nullptr;
+  size_t partials_cap = 0;
+  unsigned *counter = nullptr;
+  lmb::CGState *st_dev = nullptr;
+  lmb::CGState *st_host = nullptr;  // pinned
+  double *dot_host = nullptr;       // pinned
+  std::string err;
+};
+
+namespace lmb {
+
+inline int fail(lmb_ctx *ctx, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (ctx) ctx->err = buf;
+  return code;
+}
+
+#define LMB_CUDA(ctx, call)                                                              \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return ::lmb::fail(ctx, LMB_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                         __FILE__, __LINE__);                                            \
+  } while (0)
+
+#define LMB_CHECK_LAUNCH(ctx)                                                             \
+  do {                                                                                    \
+    cudaError_t e_ = cudaGetLastError();                                                  \
+    if (e_ != cudaSuccess)                                                                \
+      return ::lmb::fail(ctx, LMB_ERR_CUDA, "kernel launch: %s (%s:%d)", cudaGetErrorString(e_), \
+                         __FILE__, __LINE__);                                             \
+  } while (0)
+
+// named workspace, grown on demand (never shrinks until lmb_destroy)
+inline void *workspace(lmb_ctx *ctx, const std::string &name, size_t bytes) {
+  auto it = ctx->buffers.find(name);
+  if (it != ctx->buffers.end() && it->second.second >= bytes) return it->second.first;
+  if (it != ctx->buffers.end()) {
+    cudaFree(it->second.first);
+    ctx->buffers.erase(it);
+  }
+  void *p = nullptr;
+  if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+  ctx->buffers[name] = {p, bytes};
+  return p;
+}
+
+inline bool ensure_partials(lmb_ctx *ctx, size_t blocks, int nval) {
+  const size_t need = blocks * (size_t)nval;
+  if (ctx->partials_cap >= need) return true;
+  if (ctx->partials) cudaFree(ctx->partials);
+  ctx->partials = nullptr;
+  ctx->partials_cap = 0;
+  if (cudaMalloc(&ctx->partials, need * sizeof(double)) != cudaSuccess) return false;
+  ctx->partials_cap = need;
+  return true;
+}
+
+template <int P, int NC>
+inline bool make_field(lmb_ctx *ctx, const std::string &name, Field<P, NC> &f) {
+  const int64_t V = ctx->g.V;
+  f.V = V;
+  const size_t nb = Field<P, NC>::bytes(V), mb = Field<P, NC>::norm_bytes(V);
+  void *p = workspace(ctx, name, nb + mb + 256);
+  if (!p) return false;
+  f.data = (decltype(f.data))p;
+  f.norm = mb ? (float *)((char *)p + ((nb + 255) / 256) * 256) : nullptr;
+  return true;
+}
+
+inline unsigned grid_for(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+}  // namespace lmb

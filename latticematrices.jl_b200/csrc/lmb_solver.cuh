@@ -1,0 +1,282 @@
+// lmb_solver.cuh -- conjugate gradient on D^+D with device-resident scalars.
+//
+// Algorithm: cg! of the reference (cg.jl:73-137): stop when
+// |r| <= max(atol, rtol |b|), report converged / maximum_iterations /
+// nonpositive_curvature / numerical_breakdown.  One iteration is three
+// kernels, all scalars (alpha, beta, |r|^2) stay on the GPU:
+//   K1  tmp = D p                       and  pAp = |tmp|^2 = <p, D^+D p>
+//   K2  Ap  = D^+ tmp (never stored):   x += alpha p,  r -= alpha Ap,  rr = |r|^2
+//   K3  p   = r + beta p
+// The last block of each reducing kernel computes the next scalar.  When a
+// finishing condition is met the state leaves RUNNING and every later kernel
+// returns at entry, so the host may enqueue several iterations between
+// checks without changing the arithmetic.
+//
+// Mixed precision (Clark et al., "Solving lattice QCD systems of equations
+// using mixed precision solvers on GPUs", CPC 181 (2010) 1517): K1-K3 run on
+// FP32 or int16 fields, x_low accumulates in FP32; when |r_low| < delta *
+// max|r| since the last update (or |r_low| reaches the tolerance), the state
+// pauses with RELIABLE and the host performs a reliable update in FP64:
+// x += x_low, x_low = 0, r = b - D^+D x, r_low = r, rr = |r|^2.  Only the
+// FP64 true residual decides convergence.
+#pragma once
+#include "lmb_wilson.cuh"
+
+namespace lmb {
+
+enum CGStatus {
+  ST_RUNNING = 0,
+  ST_RELIABLE = 1,
+  ST_CONVERGED = 2,
+  ST_MAXITER = 3,
+  ST_NONPOSITIVE = 4,
+  ST_BREAKDOWN = 5
+};
+
+struct CGState {
+  double rr;        // |r|^2 of the iterated residual
+  double pAp, alpha, beta;
+  double tol2;      // max(atol, rtol |b|)^2
+  double maxrr;     // max |r|^2 since the last reliable update
+  double delta2;    // delta^2 (0 = plain CG, no reliable updates)
+  double rr_true;   // last FP64 true residual |b - D^+D x|^2
+  double rr_pending;
+  double bb;
+  int iter;
+  int maxiter;
+  int status;
+  int reliable_updates;
+};
+
+LMB_D void finalize_pAp(CGState *st, double pAp) {
+  st->pAp = pAp;
+  if (!isfinite(pAp)) st->status = ST_BREAKDOWN;
+  else if (pAp <= 0.0) st->status = ST_NONPOSITIVE;
+  else st->alpha = st->rr / pAp;
+}
+
+LMB_D void finalize_rr(CGState *st, double rr_new) {
+  if (!isfinite(rr_new) || rr_new < 0.0) {
+    st->iter++;
+    st->status = ST_BREAKDOWN;
+    return;
+  }
+  if (st->delta2 > 0.0) {
+    if (rr_new <= st->tol2 || rr_new < st->delta2 * st->maxrr) {
+      st->rr_pending = rr_new;
+      st->status = ST_RELIABLE;
+      return;
+    }
+    st->maxrr = fmax(st->maxrr, rr_new);
+  }
+  st->iter++;
+  if (st->delta2 == 0.0 && rr_new <= st->tol2) {
+    st->rr = rr_new;
+    st->status = ST_CONVERGED;
+    return;
+  }
+  st->beta = rr_new / st->rr;
+  st->rr = rr_new;
+  if (st->iter >= st->maxiter) st->status = ST_MAXITER;
+}
+
+// mode 0: initial residual, 1: reliable update, 2: report only
+LMB_D void finalize_true(CGState *st, double rr_true, int mode) {
+  st->rr_true = rr_true;
+  if (mode == 2) return;
+  if (!isfinite(rr_true) || rr_true < 0.0) {
+    st->status = ST_BREAKDOWN;
+    return;
+  }
+  if (mode == 1) {
+    st->iter++;
+    st->reliable_updates++;
+  }
+  if (rr_true <= st->tol2) {
+    st->rr = rr_true;
+    st->status = ST_CONVERGED;
+    return;
+  }
+  if (mode == 1) st->beta = rr_true / st->rr;
+  st->rr = rr_true;
+  st->maxrr = rr_true;
+  st->status = (st->iter >= st->maxiter) ? ST_MAXITER : ST_RUNNING;
+}
+
+template <typename R>
+LMB_D double sum_norm2(const Cx<R> *v, int n) {
+  double s = 0;
+#pragma unroll
+  for (int k = 0; k < 12; k++)
+    if (k < n) s += (double)norm2(v[k]);
+  return s;
+}
+
+// ---------------------------------------------------------------------------
+// epilogues
+// ---------------------------------------------------------------------------
+template <int PS>
+struct EpiStore {
+  Field<PS, 12> out;
+  const int *status;  // optional: skip when != RUNNING
+  LMB_D bool skip() const { return status && *(volatile const int *)status != ST_RUNNING; }
+  template <typename R> LMB_D void operator()(int s, bool active, const Cx<R> *v) const {
+    if (active) out.store(s, v);
+  }
+};
+
+template <int PS>
+struct EpiStoreNorm {  // K1
+  Field<PS, 12> out;
+  CGState *st;
+  double *partials;
+  unsigned *counter;
+  LMB_D bool skip() const { return ((volatile CGState *)st)->status != ST_RUNNING; }
+  template <typename R> LMB_D void operator()(int s, bool active, const Cx<R> *v) const {
+    double n2[1] = {0.0}, tot[1];
+    if (active) {
+      out.store(s, v);
+      n2[0] = sum_norm2(v, 12);
+    }
+    if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0)
+      finalize_pAp(st, tot[0]);
+  }
+};
+
+template <int PS, int PX>
+struct EpiCGUpdate {  // K2
+  Field<PS, 12> p, r;
+  Field<PX, 12> x;
+  CGState *st;
+  double *partials;
+  unsigned *counter;
+  LMB_D bool skip() const { return ((volatile CGState *)st)->status != ST_RUNNING; }
+  template <typename R> LMB_D void operator()(int s, bool active, const Cx<R> *v) const {
+    double n2[1] = {0.0}, tot[1];
+    if (active) {
+      const R alpha = (R)st->alpha;
+      Cx<R> pv[12], rv[12], xv[12];
+      p.load(s, pv);
+      r.load(s, rv);
+      x.load(s, xv);
+#pragma unroll
+      for (int k = 0; k < 12; k++) {
+        rv[k] = rv[k] - alpha * v[k];
+        xv[k] = xv[k] + alpha * pv[k];
+      }
+      r.store(s, rv);
+      x.store(s, xv);
+      n2[0] = sum_norm2(rv, 12);
+    }
+    if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0)
+      finalize_rr(st, tot[0]);
+  }
+};
+
+// r = b - v (FP64), r_low = r (optional), |r|^2 -> finalize_true(mode)
+template <int PS>
+struct EpiTrueResidual {
+  Field<PREC_DOUBLE, 12> b, r;
+  Field<PS, 12> r_low;
+  int write_low;
+  int mode;
+  CGState *st;
+  double *partials;
+  unsigned *counter;
+  LMB_D bool skip() const { return false; }
+  template <typename R> LMB_D void operator()(int s, bool active, const Cx<R> *v) const {
+    double n2[1] = {0.0}, tot[1];
+    if (active) {
+      Cx<double> bv[12], rv[12];
+      b.load(s, bv);
+#pragma unroll
+      for (int k = 0; k < 12; k++) rv[k] = Cx<double>(bv[k].re - (double)v[k].re, bv[k].im - (double)v[k].im);
+      r.store(s, rv);
+      if (write_low) r_low.store(s, rv);
+      n2[0] = sum_norm2(rv, 12);
+    }
+    if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0)
+      finalize_true(st, tot[0], mode);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// vector kernels
+// ---------------------------------------------------------------------------
+constexpr int kBlasThreads = 256;
+
+// K3: p = r + beta p
+template <int PS, int NC>
+__global__ void __launch_bounds__(kBlasThreads)
+    cg_p_update_kernel(Field<PS, NC> p, const Field<PS, NC> r, const CGState *st, int64_t V) {
+  if (((volatile const CGState *)st)->status != ST_RUNNING) return;
+  const int64_t s = (int64_t)blockIdx.x * kBlasThreads + threadIdx.x;
+  if (s >= V) return;
+  typedef typename Real<PS>::type R;
+  const R beta = (R)st->beta;
+  Cx<R> pv[NC], rv[NC];
+  p.load(s, pv);
+  r.load(s, rv);
+#pragma unroll
+  for (int k = 0; k < NC; k++) pv[k] = rv[k] + beta * pv[k];
+  p.store(s, pv);
+}
+
+// dst = src (precision conversion)
+template <int PD, int PSRC, int NC>
+__global__ void __launch_bounds__(kBlasThreads)
+    convert_kernel(Field<PD, NC> dst, const Field<PSRC, NC> src, int64_t V) {
+  const int64_t s = (int64_t)blockIdx.x * kBlasThreads + threadIdx.x;
+  if (s >= V) return;
+  typedef typename Real<PD>::type RD;
+  typedef typename Real<PSRC>::type RS;
+  Cx<RS> a[NC];
+  Cx<RD> b[NC];
+  src.load(s, a);
+#pragma unroll
+  for (int k = 0; k < NC; k++) b[k] = Cx<RD>((RD)a[k].re, (RD)a[k].im);
+  dst.store(s, b);
+}
+
+// x64 += x_low; x_low = 0
+template <int PX, int NC>
+__global__ void __launch_bounds__(kBlasThreads)
+    fold_kernel(Field<PREC_DOUBLE, NC> x, Field<PX, NC> xl, int64_t V) {
+  const int64_t s = (int64_t)blockIdx.x * kBlasThreads + threadIdx.x;
+  if (s >= V) return;
+  typedef typename Real<PX>::type RX;
+  Cx<double> a[NC];
+  Cx<RX> b[NC], z[NC];
+  x.load(s, a);
+  xl.load(s, b);
+#pragma unroll
+  for (int k = 0; k < NC; k++) {
+    a[k] = Cx<double>(a[k].re + (double)b[k].re, a[k].im + (double)b[k].im);
+    z[k] = Cx<RX>(0, 0);
+  }
+  x.store(s, a);
+  xl.store(s, z);
+}
+
+// |a|^2 into st->bb and the tolerance
+template <int NC>
+__global__ void __launch_bounds__(kBlasThreads)
+    norm_b_kernel(const Field<PREC_DOUBLE, NC> a, CGState *st, int64_t V, double rtol, double atol,
+                  double *partials, unsigned *counter) {
+  const int64_t s = (int64_t)blockIdx.x * kBlasThreads + threadIdx.x;
+  double n2[1] = {0.0}, tot[1];
+  if (s < V) {
+    Cx<double> v[NC];
+    a.load(s, v);
+#pragma unroll
+    for (int k = 0; k < NC; k++) n2[0] += norm2(v[k]);
+  }
+  if (grid_reduce<kBlasThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0) {
+    st->bb = tot[0];
+    const double bn = sqrt(tot[0]);
+    const double tol = fmax(atol, rtol * bn);
+    st->tol2 = tol * tol;
+  }
+}
+
+}  // namespace lmb

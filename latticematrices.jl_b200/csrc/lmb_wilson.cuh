@@ -1,0 +1,202 @@
+// lmb_wilson.cuh -- Wilson and Wilson-clover stencil on CUDA cores.
+//
+// One thread owns one lattice site.  Per direction it loads the neighbouring
+// 12-component spinor, projects it to a half spinor with (1 -/+ gamma_mu),
+// multiplies the two colour vectors by U_mu(x) (forward) or U_mu(x-mu)^+
+// (backward) and reconstructs into the 12-component accumulator.  The
+// projector/reconstruction table is the chiral-basis one of the reference
+// (WilsonDiracOperator.jl:157-263, Operators.jl:44-66):
+//   D psi = A(x) psi(x) - kappa sum_mu [U_mu(x)(1 - g_mu)psi(x+mu)
+//                                       + U_mu(x-mu)^+ (1 + g_mu) psi(x-mu)]
+// where A = 1 for plain Wilson and A = 1 - kappa cSW sum_{mu<nu} g_mu g_nu F_mu_nu
+// for Wilson-clover (WilsonDiracCloverOperator.jl:481-559).  D^+ swaps the
+// projector signs and keeps A (A is Hermitian).
+//
+// The kernel is templated on the storage precision of the input spinor, the
+// links and the clover blocks, and on an epilogue that consumes the 12 output
+// components (plain store, store + |out|^2, or a fused CG update).
+#pragma once
+#include "lmb_common.cuh"
+
+namespace lmb {
+
+constexpr int kDslashThreads = 128;
+
+// half-spin projection rows of (1 + PM g_mu) psi (WilsonDiracOperator.jl:157-175)
+template <int PM, int MU, typename R>
+LMB_D void project(const Cx<R> *p, Cx<R> *h) {
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const Cx<R> s1 = p[c], s2 = p[c + 3], s3 = p[c + 6], s4 = p[c + 9];
+    if (MU == 0) {
+      h[c] = PM > 0 ? s1 - mul_i(s4) : s1 + mul_i(s4);
+      h[c + 3] = PM > 0 ? s2 - mul_i(s3) : s2 + mul_i(s3);
+    } else if (MU == 1) {
+      h[c] = PM > 0 ? s1 - s4 : s1 + s4;
+      h[c + 3] = PM > 0 ? s2 + s3 : s2 - s3;
+    } else if (MU == 2) {
+      h[c] = PM > 0 ? s1 - mul_i(s3) : s1 + mul_i(s3);
+      h[c + 3] = PM > 0 ? s2 + mul_i(s4) : s2 - mul_i(s4);
+    } else {
+      h[c] = PM > 0 ? s1 - s3 : s1 + s3;
+      h[c + 3] = PM > 0 ? s2 - s4 : s2 + s4;
+    }
+  }
+}
+
+// accumulate the full spinor rebuilt from a half spinor
+// (WilsonDiracOperator.jl:225-263)
+template <int PM, int MU, typename R>
+LMB_D void reconstruct(Cx<R> *acc, const Cx<R> *h) {
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const Cx<R> h0 = h[c], h1 = h[c + 3];
+    acc[c] = acc[c] + h0;
+    acc[c + 3] = acc[c + 3] + h1;
+    if (MU == 0) {
+      acc[c + 6] = PM > 0 ? acc[c + 6] + mul_i(h1) : acc[c + 6] - mul_i(h1);
+      acc[c + 9] = PM > 0 ? acc[c + 9] + mul_i(h0) : acc[c + 9] - mul_i(h0);
+    } else if (MU == 1) {
+      acc[c + 6] = PM > 0 ? acc[c + 6] + h1 : acc[c + 6] - h1;
+      acc[c + 9] = PM > 0 ? acc[c + 9] - h0 : acc[c + 9] + h0;
+    } else if (MU == 2) {
+      acc[c + 6] = PM > 0 ? acc[c + 6] + mul_i(h0) : acc[c + 6] - mul_i(h0);
+      acc[c + 9] = PM > 0 ? acc[c + 9] - mul_i(h1) : acc[c + 9] + mul_i(h1);
+    } else {
+      acc[c + 6] = PM > 0 ? acc[c + 6] - h0 : acc[c + 6] + h0;
+      acc[c + 9] = PM > 0 ? acc[c + 9] - h1 : acc[c + 9] + h1;
+    }
+  }
+}
+
+// out[r + 3*half] = sum_k U(r,k) h[k + 3*half], U column-major (u[r + 3k])
+template <typename R>
+LMB_D void su3_mul_half(const Cx<R> *u, const Cx<R> *h, Cx<R> *o) {
+#pragma unroll
+  for (int half = 0; half < 2; half++)
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+      Cx<R> v = u[r] * h[3 * half];
+      v = cfma(u[r + 3], h[3 * half + 1], v);
+      v = cfma(u[r + 6], h[3 * half + 2], v);
+      o[r + 3 * half] = v;
+    }
+}
+// U^+ : (U^+)(r,k) = conj(U(k,r)) = conj(u[k + 3r])
+template <typename R>
+LMB_D void su3_adj_mul_half(const Cx<R> *u, const Cx<R> *h, Cx<R> *o) {
+#pragma unroll
+  for (int half = 0; half < 2; half++)
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+      Cx<R> v = conj(u[3 * r]) * h[3 * half];
+      v = cfma_conj(u[3 * r + 1], h[3 * half + 1], v);
+      v = cfma_conj(u[3 * r + 2], h[3 * half + 2], v);
+      o[r + 3 * half] = v;
+    }
+}
+
+template <typename R>
+LMB_D void scale_phase(Cx<R> *h, int n, const double *ph) {
+  const Cx<R> f((R)ph[0], (R)ph[1]);
+#pragma unroll
+  for (int k = 0; k < 6; k++)
+    if (k < n) h[k] = h[k] * f;
+}
+
+// Hermitian 6x6 (packed: 6 real diagonal, 15 complex lower triangle in row
+// order) times a 6-vector
+template <typename R>
+LMB_D void herm6_mul(const R *a, const Cx<R> *v, Cx<R> *o) {
+#pragma unroll
+  for (int i = 0; i < 6; i++) o[i] = a[i] * v[i];
+  int k = 6;
+#pragma unroll
+  for (int i = 1; i < 6; i++)
+#pragma unroll
+    for (int j = 0; j < i; j++) {
+      const Cx<R> aij(a[k], a[k + 1]);  // A[i][j]; A[j][i] = conj
+      o[i] = cfma(aij, v[j], o[i]);
+      o[j] = cfma_conj(aij, v[i], o[j]);
+      k += 2;
+    }
+}
+
+// hopping term of one direction, forward and backward, accumulated into acc
+template <typename R, int DAG, int MU, class SF, class G>
+LMB_D void hop_dir(const Geom &g, int s, const int *c, const SF &in, const G &U,
+                   Cx<R> *acc) {
+  // D: forward (1 - g), backward (1 + g);  D^+: swapped
+  constexpr int FPM = DAG ? +1 : -1;
+  constexpr int BPM = -FPM;
+  Cx<R> p[12], h[6], uh[6], u[9];
+  int wrap;
+  {
+    const int sp = fwd_site(g, s, c, MU, 1, &wrap);
+    in.load(sp, p);
+    project<FPM, MU>(p, h);
+    if (wrap && ((g.phase_mask >> MU) & 1)) scale_phase(h, 6, g.ph_fwd[MU]);
+    U.load(MU, s, u);
+    su3_mul_half(u, h, uh);
+    reconstruct<FPM, MU>(acc, uh);
+  }
+  {
+    const int sm = bwd_site(g, s, c, MU, 1, &wrap);
+    in.load(sm, p);
+    project<BPM, MU>(p, h);
+    if (wrap && ((g.phase_mask >> MU) & 1)) scale_phase(h, 6, g.ph_bwd[MU]);
+    U.load(MU, sm, u);
+    su3_adj_mul_half(u, h, uh);
+    reconstruct<BPM, MU>(acc, uh);
+  }
+}
+
+// no-op clover for plain Wilson
+struct NoClover {
+  int64_t V;
+};
+
+// The Wilson(-clover) kernel.  Epi must provide:
+//   bool skip() const                      -- whole grid exits (paused solve)
+//   void operator()(s, active, out[12])    -- consume the result
+template <typename R, int DAG, bool CLOVER, class SF, class G, class CL, class Epi>
+__global__ void __launch_bounds__(kDslashThreads)
+    wilson_dslash_kernel(const Geom g, const SF in, const G U, const CL A,
+                         const R kappa, Epi epi) {
+  if (epi.skip()) return;
+  const int s = blockIdx.x * kDslashThreads + threadIdx.x;
+  const bool active = s < g.V;
+  Cx<R> out[12];
+  if (active) {
+    int c[4];
+    site_coords(g, s, c);
+    Cx<R> acc[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) acc[k] = Cx<R>(0, 0);
+    hop_dir<R, DAG, 0>(g, s, c, in, U, acc);
+    hop_dir<R, DAG, 1>(g, s, c, in, U, acc);
+    hop_dir<R, DAG, 2>(g, s, c, in, U, acc);
+    hop_dir<R, DAG, 3>(g, s, c, in, U, acc);
+    Cx<R> p[12];
+    in.load(s, p);
+    if constexpr (CLOVER) {
+      R a[36];
+      Cx<R> v[6], o[6];
+#pragma unroll
+      for (int blk = 0; blk < 2; blk++) {
+        A.load(blk, s, a);
+#pragma unroll
+        for (int k = 0; k < 6; k++) v[k] = p[6 * blk + k];
+        herm6_mul(a, v, o);
+#pragma unroll
+        for (int k = 0; k < 6; k++) out[6 * blk + k] = o[k] - kappa * acc[6 * blk + k];
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 12; k++) out[k] = p[k] - kappa * acc[k];
+    }
+  }
+  epi(s, active, out);
+}
+
+}  // namespace lmb

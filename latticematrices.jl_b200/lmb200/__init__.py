@@ -1,0 +1,17 @@
+"""lmb200 -- the LatticeMatrices.jl Dirac-operator / D'D-CG path on B200.
+
+Host-side mirror of the reference's operator API over liblmb200.so (C ABI in
+include/lmb200.h).  Julia names map as `mul!` -> `mul_`, `cg!` -> `cg_`,
+`solve!` -> `solve_`, `update_clover!` -> `update_clover_`, `D'` ->
+`adjoint(D)`.
+"""
+from ._lib import ArgumentError, LMBError, load, EXPORTED, LIB_PATH  # noqa: F401
+from .lattice import (LatticeMatrix, clear_matrix_, halo_is_dirty,  # noqa: F401
+                      mark_halo_dirty_, similar, substitute_)
+from .operators import (CloverFieldStrength4D, WilsonDiracCloverOperator4D,  # noqa: F401
+                        WilsonDiracOperator4D, adjoint, mul_,
+                        mul_cached_clover_, mul_cached_clover_adjoint_,
+                        update_clover_)
+from .inputs import gaussian_fermion, random_su3_links  # noqa: F401
+from .solver import (CGResult, DdagDOp, cg_, dot, pseudofermion_action,  # noqa: F401
+                     solve_)

@@ -1,0 +1,244 @@
+"""Dirac operators behind the reference's operator API.
+
+`mul_(out, D, psi)` is Julia's `mul!(out, D, psi)`; `adjoint(D)` gives the
+adjoint operator as `D'` does.  Every application calls liblmb200 through its
+C ABI on the device pointers of the LatticeMatrix storage; the operator keeps
+its own lmb_ctx, which caches the repacked links and the clover blocks keyed
+by link identity and core epoch (CloverCacheState,
+WilsonDiracCloverOperator.jl:418-432).
+"""
+from __future__ import annotations
+
+import ctypes
+
+from ._lib import (ArgumentError, Context, LINKS_THIN, PREC)
+from .lattice import LatticeMatrix, mark_halo_dirty_
+
+_NC_SUPPORTED = 3
+
+
+def _stream():
+    import torch
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _validate_links(U, what="gauge link"):
+    if len(U) != 4:
+        raise ArgumentError("U must be a vector of length 4")
+    ref = U[0]
+    if ref.NC1 != ref.NC2:
+        raise ArgumentError("gauge links must be square matrices")
+    for mu, link in enumerate(U, start=1):
+        if (link.NC1, link.NC2) != (ref.NC1, ref.NC2):
+            raise ArgumentError("all gauge links must have the same matrix size")
+        if link.gsize != ref.gsize:
+            raise ArgumentError("all gauge links must have the same global lattice size")
+        if link.nw != ref.nw:
+            raise ArgumentError("all gauge links must have the same halo width")
+        if any(p != 1 for p in link.phases):
+            raise ArgumentError(f"{what} U[{mu}] must use periodic boundary phases")
+        if link.elementtype != ref.elementtype:
+            raise ArgumentError("all gauge links must have the same element type")
+
+
+def _validate_application(result, U, psi, nc2):
+    if result is psi:
+        raise ArgumentError("mul! requires distinct result and input fields")
+    if not result.same_geometry(psi):
+        raise ArgumentError("result and fermion fields must use the same lattice geometry")
+    if result.phases != psi.phases:
+        raise ArgumentError("result and fermion fields must use the same boundary phases")
+    if psi.NC2 != nc2 or result.NC2 != nc2:
+        raise ArgumentError(f"fermion fields must have {nc2} spin components per site")
+    for mu, link in enumerate(U, start=1):
+        if link.NC1 != psi.NC1:
+            raise ArgumentError(
+                f"gauge link U[{mu}] and fermion field have different color sizes")
+        if link.elementtype != psi.elementtype:
+            raise ArgumentError(
+                f"gauge link U[{mu}] and fermion field have different element types")
+        if link.gsize != psi.gsize or link.nw != psi.nw:
+            raise ArgumentError(
+                f"gauge link U[{mu}] and fermion field use different lattice geometry")
+    if psi.NC1 != _NC_SUPPORTED:
+        raise ArgumentError(
+            f"the sm_100a kernels implement NC={_NC_SUPPORTED}; got NC={psi.NC1}")
+
+
+class _Adjoint:
+    def __init__(self, parent):
+        self.parent = parent
+
+
+def adjoint(op):
+    """`op'`: adjoint wrapper; adjoint(adjoint(op)) is op."""
+    if isinstance(op, _Adjoint):
+        return op.parent
+    if hasattr(op, "adjoint"):
+        return op.adjoint()
+    return _Adjoint(op)
+
+
+class _LinkOperator:
+    """Shared machinery: context, geometry and link upload."""
+
+    def __init__(self, U):
+        _validate_links(U)
+        self.U = list(U)
+        self._ctx = None
+
+    @property
+    def ctx(self) -> Context:
+        if self._ctx is None:
+            dev = self.U[0].A.device
+            self._ctx = Context(dev.index or 0)
+        return self._ctx
+
+    def _bind(self, psi, stream):
+        ctx = self.ctx
+        ctx.set_geometry(psi.gsize, psi.nw, psi.phases, psi.coords,
+                         psi.dtype_code)
+        ctx.upload_links(LINKS_THIN, [u.data_ptr() for u in self.U],
+                         [u.halo_epoch.core for u in self.U], stream)
+        return ctx
+
+
+class WilsonDiracOperator4D(_LinkOperator):
+    """Wilson operator (WilsonDiracOperator.jl:1-76)."""
+
+    def __init__(self, U, kappa):
+        if len(U) != 4:
+            raise ArgumentError("U must be a vector of length 4.")
+        super().__init__(U)
+        self.kappa = float(kappa)
+
+    def adjoint(self):
+        return AdjointWilsonDiracOperator4D(self)
+
+    def _apply(self, out, psi, dagger, precision):
+        _validate_application(out, self.U, psi, 4)
+        st = _stream()
+        ctx = self._bind(psi, st)
+        ctx.check(ctx.lib.lmb_wilson_apply(
+            ctx.handle, out.data_ptr(), psi.data_ptr(), self.kappa,
+            int(dagger), PREC[precision], st))
+        mark_halo_dirty_(out)
+        return out
+
+
+class AdjointWilsonDiracOperator4D(_Adjoint):
+    def _apply(self, out, psi, dagger, precision):
+        return self.parent._apply(out, psi, not dagger, precision)
+
+
+class CloverFieldStrength4D:
+    """The six anti-Hermitian clover components (12,13,14,23,24,34)
+    (WilsonDiracCloverOperator.jl:15-35)."""
+
+    def __init__(self, operator):
+        self.operator = operator
+        self.components = None
+
+    def refresh(self, psi_template):
+        op = self.operator
+        U = op.wilson.U
+        st = _stream()
+        ctx = op.wilson._bind(psi_template, st)
+        comps = [U[0].similar() for _ in range(6)]
+        arr = (ctypes.c_void_p * 6)(*[c.data_ptr() for c in comps])
+        ctx.check(ctx.lib.lmb_clover_field_strength(ctx.handle, arr, st))
+        for c in comps:
+            mark_halo_dirty_(c)
+        self.components = comps
+        return self
+
+    def __getitem__(self, i):
+        return self.components[i]
+
+    def __len__(self):
+        return 6
+
+
+class WilsonDiracCloverOperator4D:
+    """D = D_W - kappa cSW sum_{mu<nu} g_mu g_nu F_mu_nu
+    (WilsonDiracCloverOperator.jl:401-456)."""
+
+    def __init__(self, U, kappa, cSW):
+        self.wilson = WilsonDiracOperator4D(U, kappa)
+        self.cSW = float(cSW)
+        self.clover = CloverFieldStrength4D(self)
+
+    @property
+    def kappa(self):
+        return self.wilson.kappa
+
+    @property
+    def U(self):
+        return self.wilson.U
+
+    @property
+    def ctx(self):
+        return self.wilson.ctx
+
+    def adjoint(self):
+        return AdjointWilsonDiracCloverOperator4D(self)
+
+    def field_strength(self, psi_template=None):
+        """Refresh and return the CloverFieldStrength4D components."""
+        tmpl = psi_template
+        if tmpl is None:
+            tmpl = LatticeMatrix(3, 4, 4, self.U[0].gsize, nw=self.U[0].nw,
+                                 elementtype=self.U[0].elementtype,
+                                 device=self.U[0].A.device)
+        return self.clover.refresh(tmpl)
+
+    def _apply(self, out, psi, dagger, precision):
+        _validate_application(out, self.U, psi, 4)
+        st = _stream()
+        ctx = self.wilson._bind(psi, st)
+        ctx.check(ctx.lib.lmb_wilson_clover_apply(
+            ctx.handle, out.data_ptr(), psi.data_ptr(), self.kappa, self.cSW,
+            int(dagger), PREC[precision], st))
+        mark_halo_dirty_(out)
+        return out
+
+
+class AdjointWilsonDiracCloverOperator4D(_Adjoint):
+    def _apply(self, out, psi, dagger, precision):
+        return self.parent._apply(out, psi, not dagger, precision)
+
+
+def update_clover_(operator, U=None):
+    """update_clover!(operator[, U]) (WilsonDiracCloverOperator.jl:458-479).
+    The link cache is keyed by link identity and core epoch, so a refresh
+    only needs the new references."""
+    if U is not None:
+        _validate_links(U)
+        operator.wilson.U[:] = list(U)
+    return operator
+
+
+def mul_(out, operator, psi, precision="double"):
+    """mul!(out, operator, psi).  precision: "double" (the reference's
+    arithmetic), or "single" / "half" storage for the inner solver."""
+    if precision not in PREC:
+        raise ArgumentError(f"unknown precision {precision!r}")
+    if hasattr(operator, "_apply"):
+        return operator._apply(out, psi, False, precision)
+    if hasattr(operator, "mul_"):
+        return operator.mul_(out, psi)
+    raise ArgumentError(f"no mul! method for {type(operator).__name__}")
+
+
+def mul_cached_clover_(result, cache, U1, U2, U3, U4, psi):
+    """mul_cached_clover!(result, cache, U1, U2, U3, U4, psi)
+    (WilsonDiracCloverOperator.jl:627-651): links given explicitly; the
+    cached clover blocks are rebuilt when their identity or epoch changes."""
+    update_clover_(cache, [U1, U2, U3, U4])
+    return mul_(result, cache, psi)
+
+
+def mul_cached_clover_adjoint_(result, cache, U1, U2, U3, U4, psi):
+    """mul_cached_clover_adjoint! (WilsonDiracCloverOperator.jl:653-668)."""
+    update_clover_(cache, [U1, U2, U3, U4])
+    return mul_(result, adjoint(cache), psi)

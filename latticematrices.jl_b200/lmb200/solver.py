@@ -1,0 +1,226 @@
+"""CG on D'D behind the reference's solver API (LinearAlgebras/cg.jl,
+Operators/DiracOperators.jl).
+
+`cg_(x, DdagDOp(D, temp), b, r, p, Ap; ...)` with a Wilson or Wilson-clover D
+runs the whole solve in liblmb200 (lmb_cg_ddagd): stencils, vector updates and
+reductions on the GPU, scalars on the GPU, FP64 throughout by default or an
+FP32 / int16 inner solve with FP64 reliable updates (precision="single" /
+"half").  Any other operator (a user-defined one with `mul_`) runs the
+reference's generic loop (cg.jl:73-137) on device tensors.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass
+
+from ._lib import (ArgumentError, CG_REASONS, CGParams, CGResultC, PREC,
+                   OP_WILSON, OP_WILSON_CLOVER)
+from .lattice import LatticeMatrix, mark_halo_dirty_
+from .operators import (WilsonDiracCloverOperator4D, WilsonDiracOperator4D,
+                        _stream, adjoint, mul_)
+
+
+@dataclass
+class CGResult:
+    """CGResult (cg.jl:1-13)."""
+    converged: bool
+    iterations: int
+    residual_norm: float
+    relative_residual: float
+    reason: str
+    reliable_updates: int = 0
+    true_residual_norm: float = float("nan")
+    dslash_ms: float = 0.0
+    update_ms: float = 0.0
+    dslash_launches: int = 0
+    update_launches: int = 0
+    kernel_launches: int = 0
+
+
+class DdagDOp:
+    """D' D with a caller-owned temporary (DiracOperators.jl:93-121)."""
+
+    def __init__(self, D, temp=None):
+        self.D = D
+        self.temp = temp
+
+    def adjoint(self):
+        return self
+
+    def mul_(self, y, x):
+        if self.temp is None:
+            raise ArgumentError("DdagDOp needs a temporary field")
+        if self.temp is x or self.temp is y:
+            raise ArgumentError(
+                "DdagDOp temporary field must not alias its input or output")
+        mul_(self.temp, self.D, x)
+        mul_(y, adjoint(self.D), self.temp)
+        return y
+
+
+def _validate_cg_arguments(x, b, r, p, Ap, rtol, atol, maxiter):
+    # cg.jl:33-47
+    fields = (x, b, r, p, Ap)
+    names = ("x", "b", "r", "p", "Ap")
+    for i in range(len(fields)):
+        for j in range(i + 1, len(fields)):
+            if fields[i] is not None and fields[i] is fields[j]:
+                raise ArgumentError(
+                    f"CG fields {names[i]} and {names[j]} must not alias")
+    if not rtol >= 0:
+        raise ArgumentError("rtol must be nonnegative")
+    if not atol >= 0:
+        raise ArgumentError("atol must be nonnegative")
+    if not math.isfinite(rtol):
+        raise ArgumentError("rtol must be finite")
+    if not math.isfinite(atol):
+        raise ArgumentError("atol must be finite")
+    if maxiter < 0:
+        raise ArgumentError("maxiter must be nonnegative")
+
+
+def _native_operator(A):
+    if not isinstance(A, DdagDOp):
+        return None
+    D = A.D
+    if isinstance(D, WilsonDiracCloverOperator4D):
+        return D, OP_WILSON_CLOVER
+    if isinstance(D, WilsonDiracOperator4D):
+        return D, OP_WILSON
+    return None
+
+
+def cg_(x, A, b, r=None, p=None, Ap=None, *, rtol=1e-10, atol=0.0,
+        maxiter=5000, precision="double", delta=0.1, check_interval=0,
+        profile=False):
+    """cg!(x, A, b, r, p, Ap; rtol, atol, maxiter) -> CGResult."""
+    _validate_cg_arguments(x, b, r, p, Ap, rtol, atol, maxiter)
+    if precision not in PREC:
+        raise ArgumentError(f"unknown precision {precision!r}")
+    native = _native_operator(A)
+    if native is not None:
+        D, op = native
+        wilson = D.wilson if op == OP_WILSON_CLOVER else D
+        prm = CGParams()
+        prm.op = op
+        prm.kappa = D.kappa
+        prm.csw = getattr(D, "cSW", 0.0)
+        prm.rtol, prm.atol, prm.maxiter = float(rtol), float(atol), int(maxiter)
+        prm.precision = PREC[precision]
+        prm.delta = float(delta)
+        prm.check_interval = int(check_interval)
+        prm.profile = int(bool(profile))
+        st = _stream()
+        ctx = wilson._bind(b, st)
+        res = CGResultC()
+        ctx.check(ctx.lib.lmb_cg_ddagd(ctx.handle, ctypes.byref(prm),
+                                       x.data_ptr(), b.data_ptr(),
+                                       ctypes.byref(res), st))
+        mark_halo_dirty_(x)
+        return CGResult(bool(res.converged), res.iterations, res.residual_norm,
+                        res.relative_residual, CG_REASONS[res.reason],
+                        res.reliable_updates, res.true_residual_norm,
+                        res.dslash_ms, res.update_ms, res.dslash_launches,
+                        res.update_launches, res.kernel_launches)
+    if precision != "double":
+        raise ArgumentError("mixed precision needs a native DdagDOp operator")
+    return _cg_generic(x, A, b, r, p, Ap, rtol, atol, maxiter)
+
+
+def _rdot(a: LatticeMatrix, b: LatticeMatrix) -> float:
+    return float((a.core_view().conj() * b.core_view()).sum().real)
+
+
+def _axpby(a, X, b, Y):
+    Y.core_view().mul_(b).add_(X.core_view(), alpha=a)
+    mark_halo_dirty_(Y)
+
+
+def _result(conv, it, rn, bn, reason):
+    rel = (0.0 if rn == 0 else math.inf) if bn == 0 else rn / bn
+    return CGResult(conv, it, rn, rel, reason)
+
+
+def _cg_generic(x, A, b, r, p, Ap, rtol, atol, maxiter):
+    # cg.jl:73-137, line for line, for user-defined operators
+    if r is None or p is None or Ap is None:
+        raise ArgumentError("the generic CG needs caller-owned r, p, Ap")
+    bb = _rdot(b, b)
+    if not math.isfinite(bb) or bb < 0:
+        return _result(False, 0, math.nan, math.nan, "numerical_breakdown")
+    bn = math.sqrt(bb)
+    tol = max(atol, rtol * bn)
+    mul_(Ap, A, x)
+    _axpby(1, b, 0, r)
+    _axpby(-1, Ap, 1, r)
+    _axpby(1, r, 0, p)
+    rr = _rdot(r, r)
+    if not math.isfinite(rr) or rr < 0:
+        return _result(False, 0, math.nan, bn, "numerical_breakdown")
+    rn = math.sqrt(rr)
+    if rn <= tol:
+        return _result(True, 0, rn, bn, "converged")
+    for it in range(1, maxiter + 1):
+        mul_(Ap, A, p)
+        pAp = _rdot(p, Ap)
+        if not math.isfinite(pAp):
+            return _result(False, it - 1, rn, bn, "numerical_breakdown")
+        if pAp <= 0:
+            return _result(False, it - 1, rn, bn, "nonpositive_curvature")
+        alpha = rr / pAp
+        _axpby(alpha, p, 1, x)
+        _axpby(-alpha, Ap, 1, r)
+        rr_new = _rdot(r, r)
+        if not math.isfinite(rr_new) or rr_new < 0:
+            return _result(False, it, math.nan, bn, "numerical_breakdown")
+        rn = math.sqrt(rr_new)
+        if rn <= tol:
+            return _result(True, it, rn, bn, "converged")
+        beta = rr_new / rr
+        _axpby(1, r, beta, p)
+        rr = rr_new
+    return _result(False, maxiter, rn, bn, "maximum_iterations")
+
+
+def solve_(x, A, b, r=None, p=None, Ap=None, **kwargs):
+    """solve!(x, A::DdagDOp, b, r, p, Ap; kwargs...) (DiracOperators.jl:130-143)."""
+    return cg_(x, A, b, r, p, Ap, **kwargs)
+
+
+def dot(a: LatticeMatrix, b: LatticeMatrix, ctx=None) -> complex:
+    """dot(A, B) = sum conj(A) B over the core (linearalgebra_D.jl:3325-3341),
+    reduced on the GPU by lmb_field_dot."""
+    from ._lib import Context
+    if not a.same_geometry(b) or (a.NC1, a.NC2) != (b.NC1, b.NC2):
+        raise ArgumentError("dot requires fields of the same shape")
+    if a.elementtype != b.elementtype:
+        raise ArgumentError("dot requires fields of the same element type")
+    ctx = ctx or _dot_context(a)
+    ctx.set_geometry(a.gsize, a.nw, a.phases, a.coords, a.dtype_code)
+    out = (ctypes.c_double * 2)()
+    st = _stream()
+    ctx.check(ctx.lib.lmb_field_dot(ctx.handle, a.data_ptr(), b.data_ptr(),
+                                    a.NC1 * a.NC2, out, st))
+    return complex(out[0], out[1])
+
+
+_DOT_CTX = {}
+
+
+def _dot_context(a):
+    from ._lib import Context
+    dev = a.A.device.index or 0
+    if dev not in _DOT_CTX:
+        _DOT_CTX[dev] = Context(dev)
+    return _DOT_CTX[dev]
+
+
+def pseudofermion_action(D, phi, eta, Deta, r, p, Ap, **kwargs):
+    """real(dot(phi, (D'D)^-1 phi)) (DiracOperators.jl:145-163)."""
+    res = solve_(eta, DdagDOp(D, Deta), phi, r, p, Ap, **kwargs)
+    if not res.converged:
+        raise RuntimeError(
+            f"CG failed with reason {res.reason} after {res.iterations} "
+            f"iterations; relative residual = {res.relative_residual}")
+    return dot(phi, eta).real

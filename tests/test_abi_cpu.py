@@ -1,0 +1,96 @@
+"""CPU checks of the boundary: the C-ABI library loads, exports every symbol
+include/lmb200.h declares, and the host mirror validates arguments the way the
+reference does before any CUDA call."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared_symbols():
+    src = open(os.path.join(ROOT, "include", "lmb200.h")).read()
+    return sorted(set(re.findall(r"\b(lmb_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    import lmb200
+    lib = lmb200.load()
+    declared = _declared_symbols()
+    assert declared, "no declarations found"
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert sorted(lmb200.EXPORTED) == declared
+    assert lib.lmb_version() >= 100
+
+
+def _cpu_field(lmb, nc1, nc2, L=(4, 4, 4, 4), **kw):
+    return lmb.LatticeMatrix(nc1, nc2, 4, L, device="cpu", **kw)
+
+
+def test_lattice_validation():
+    import lmb200 as lmb
+    with pytest.raises(lmb.ArgumentError):
+        lmb.LatticeMatrix(3, 4, 4, (4, 4, 4, 4), nw=-1, device="cpu")
+    with pytest.raises(lmb.ArgumentError):
+        lmb.LatticeMatrix(3, 4, 4, (4, 4, 0, 4), device="cpu")
+    with pytest.raises(lmb.ArgumentError):
+        lmb.LatticeMatrix(3, 4, 4, (4, 4, 4, 4), phases=(1, 1, 0, -1),
+                          device="cpu")
+    with pytest.raises(lmb.ArgumentError):
+        lmb.LatticeMatrix(3, 4, 4, (4, 4, 2, 4), nw=3, device="cpu")
+    f = _cpu_field(lmb, 3, 4, phases=(1, 1, 1, -1))
+    arr = np.asfortranarray(np.random.default_rng(0).normal(size=(3, 4, 4, 4, 4, 4))
+                            + 0j)
+    f.set_core(arr)
+    assert np.array_equal(f.gather_matrix(), arr)
+    assert f.halo_epoch.core == 1
+    # padded storage is the Julia column-major layout
+    j = f.A.numpy()
+    assert j[1 + 2, 1 + 1, 1 + 0, 1 + 3, 2, 1] == arr[1, 2, 3, 0, 1, 2]
+
+
+def test_operator_validation_before_cuda():
+    import lmb200 as lmb
+    U = [_cpu_field(lmb, 3, 3) for _ in range(4)]
+    psi = _cpu_field(lmb, 3, 4, phases=(1, 1, 1, -1))
+    D = lmb.WilsonDiracCloverOperator4D(U, 0.12, 1.0)
+    with pytest.raises(lmb.ArgumentError, match="distinct"):
+        lmb.mul_(psi, D, psi)
+    other = _cpu_field(lmb, 3, 4, phases=(1, 1, 1, 1))
+    with pytest.raises(lmb.ArgumentError, match="boundary phases"):
+        lmb.mul_(other, D, psi)
+    bad = _cpu_field(lmb, 3, 4, L=(4, 4, 4, 8))
+    with pytest.raises(lmb.ArgumentError, match="geometry"):
+        lmb.mul_(bad, D, psi)
+    with pytest.raises(lmb.ArgumentError, match="periodic"):
+        lmb.WilsonDiracOperator4D(
+            [_cpu_field(lmb, 3, 3, phases=(1, 1, 1, -1)) for _ in range(4)], 0.1)
+    with pytest.raises(lmb.ArgumentError):
+        lmb.WilsonDiracOperator4D(U[:3], 0.1)
+    U2 = [_cpu_field(lmb, 2, 2) for _ in range(4)]
+    psi2 = _cpu_field(lmb, 2, 4)
+    with pytest.raises(lmb.ArgumentError, match="NC=3"):
+        lmb.mul_(psi2.similar(), lmb.WilsonDiracOperator4D(U2, 0.1), psi2)
+    with pytest.raises(lmb.ArgumentError):
+        lmb.mul_(psi.similar(), D, psi, precision="quad")
+    assert lmb.adjoint(lmb.adjoint(D)) is D
+
+
+def test_cg_validation_before_cuda():
+    import lmb200 as lmb
+    x = _cpu_field(lmb, 3, 4)
+    b = _cpu_field(lmb, 3, 4)
+    with pytest.raises(lmb.ArgumentError, match="alias"):
+        lmb.cg_(x, None, b, x, None, None)
+    with pytest.raises(lmb.ArgumentError, match="rtol"):
+        lmb.cg_(x, None, b, rtol=-1)
+    with pytest.raises(lmb.ArgumentError, match="maxiter"):
+        lmb.cg_(x, None, b, maxiter=-1)
+    with pytest.raises(lmb.ArgumentError, match="finite"):
+        lmb.cg_(x, None, b, atol=float("inf"))
+    D = lmb.DdagDOp(None, b)
+    with pytest.raises(lmb.ArgumentError, match="alias"):
+        D.mul_(x, b)
