@@ -35,7 +35,7 @@ def _fields(lmb, orc, L, amplitude=0.3, nw=1, phases=PHASES, dtype=np.complex128
 
 @pytest.mark.parametrize("L,nw,phases", [
     ((4, 4, 4, 4), 1, PHASES), ((3, 2, 2, 4), 0, TWISTED),
-    ((6, 4, 2, 8), 3, TWISTED), ((8, 8, 8, 8), 1, PHASES)])
+    ((6, 4, 4, 8), 3, TWISTED), ((8, 8, 8, 8), 1, PHASES)])
 @pytest.mark.parametrize("dagger", [False, True])
 def test_wilson_fp64_matches_oracle(lmb, orc, L, nw, phases, dagger):
     U, psi, Ud, pd = _fields(lmb, orc, L, nw=nw, phases=phases)
