@@ -160,6 +160,23 @@ int lmb_random_su3_links(lmb_ctx *ctx, void *const U[4], double amplitude,
 int lmb_gaussian_field(lmb_ctx *ctx, void *out, int ncomp, uint64_t seed,
                        void *stream);
 
+
+/* Inner product that allocates nothing: no reference counterpart.  The same
+ * sum as lmb_field_dot, for callers that cannot call cudaMalloc (work
+ * recorded into a CUDA graph by stream capture, pool-managed device memory
+ * near its limit, loops where an allocation would synchronise the device).
+ * No context: the geometry (L, nw, dtype as in lmb_set_geometry) is passed
+ * directly, the result (Re, Im) is written to the device array out_device[2]
+ * on `stream`, and nothing synchronises.  Scratch is a 1 MiB static device
+ * array inside the library, so one call takes at most 16,777,216 sites
+ * (LMB_ERR_ARG beyond); every call shares it, so calls that overlap on the
+ * GPU (unordered streams) race.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) -- make that first call
+ * before any stream capture. */
+int lmb_field_dot_noalloc(const void *a, const void *b, const int L[4],
+                          int nw, int dtype, int ncomp, double *out_device,
+                          void *stream);
+
 #ifdef __cplusplus
 }
 #endif

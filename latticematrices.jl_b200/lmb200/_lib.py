@@ -32,6 +32,7 @@ EXPORTED = (
     "lmb_set_geometry", "lmb_links_upload", "lmb_wilson_apply",
     "lmb_wilson_clover_apply", "lmb_clover_field_strength", "lmb_cg_ddagd",
     "lmb_field_dot", "lmb_random_su3_links", "lmb_gaussian_field",
+    "lmb_field_dot_noalloc",
 )
 
 
@@ -110,6 +111,9 @@ def load(path: str = LIB_PATH):
                                              vp]
         lib.lmb_gaussian_field.argtypes = [vp, vp, ctypes.c_int,
                                            ctypes.c_uint64, vp]
+        lib.lmb_field_dot_noalloc.argtypes = [vp, vp, ip, ctypes.c_int,
+                                              ctypes.c_int, ctypes.c_int,
+                                              vp, vp]
         for name in EXPORTED:
             if name not in ("lmb_create", "lmb_destroy", "lmb_last_error",
                             "lmb_version"):
