@@ -38,24 +38,36 @@ PHASES = (1, 1, 1, -1)
 # cSW 1.0, links exp(0.2 i H) seed 1, source seed 2, rtol 1e-10), measured by
 # the GPU FP64 solve of this file; the CPU reference arm multiplies its
 # per-iteration time by it.
-FP64_ITERATIONS_32x64 = None
+FP64_ITERATIONS_32x64 = 450
 
 # Algorithmic bytes per lattice site of the two stencil kernels of a CG
-# iteration: every operand read once, every output written once.
-#  K1  tmp = D p  (+|tmp|^2):  links 4x18 reals, clover 2x36 reals, p, tmp
+# iteration: every operand read once, every output written once, in the
+# storage format the kernel reads (links: 12 reals per SU(3) link with the
+# third row rebuilt, else 18; clover: two Hermitian 6x6 blocks = 72 reals).
+#  K1  tmp = D p  (+|tmp|^2):  links, clover, p, tmp
 #  K2  D^+ tmp fused with x += a p, r -= a Ap, |r|^2:  links, clover, tmp,
 #      p, r (read+write), x (read+write, FP32 for the mixed solves)
-SPINOR_BYTES = {"double": 192, "single": 96, "half": 52}   # 24 reals (+norm)
-GAUGE_BYTES = {"double": 576 + 576, "single": 288 + 288, "half": 144 + 144}
-X_BYTES = {"double": 192, "single": 96, "half": 96}
+REAL_BYTES = {"double": 8, "single": 4, "half": 2}
 
 
-def k1_bytes(prec):
-    return GAUGE_BYTES[prec] + 2 * SPINOR_BYTES[prec]
+def spinor_bytes(prec):
+    return 24 * REAL_BYTES[prec] + (4 if prec == "half" else 0)  # + norm
 
 
-def k2_bytes(prec):
-    return GAUGE_BYTES[prec] + 4 * SPINOR_BYTES[prec] + 2 * X_BYTES[prec]
+def gauge_bytes(prec, link_reals):
+    return (4 * link_reals + 72) * REAL_BYTES[prec]
+
+
+def x_bytes(prec):
+    return 24 * (8 if prec == "double" else 4)
+
+
+def k1_bytes(prec, link_reals=18):
+    return gauge_bytes(prec, link_reals) + 2 * spinor_bytes(prec)
+
+
+def k2_bytes(prec, link_reals=18):
+    return gauge_bytes(prec, link_reals) + 4 * spinor_bytes(prec) + 2 * x_bytes(prec)
 
 
 # Wilson-clover M: 1320 (hopping) + 504 (clover) + 48 flops per site
@@ -354,19 +366,21 @@ def run_lmb(args):
     peak, peak_kind = measured_peak()
     dominant = "K2 (D^+ tmp fused with the CG update)" if k2_ms >= k1_ms \
         else "K1 (tmp = D p with |tmp|^2)"
+    lr, lr64 = mixed.link_reals, res64_link_reals(r64)
     if k2_ms >= k1_ms:
-        per_launch_ms, bps = k2_ms / max(k2_n, 1), k2_bytes(prec)
+        per_launch_ms, bps = k2_ms / max(k2_n, 1), k2_bytes(prec, lr)
         tkey = f"k2_{prec}"
     else:
-        per_launch_ms, bps = k1_ms / max(k1_n, 1), k1_bytes(prec)
+        per_launch_ms, bps = k1_ms / max(k1_n, 1), k1_bytes(prec, lr)
         tkey = f"k1_{prec}"
     achieved = bps * sites / (per_launch_ms * 1e-3) / 1e9
     traffic = traffic_per_site().get(tkey)
-    k1_gbs = k1_bytes(prec) * sites / (k1_ms / max(k1_n, 1) * 1e-3) / 1e9
-    k2_gbs = k2_bytes(prec) * sites / (k2_ms / max(k2_n, 1) * 1e-3) / 1e9
+    k1_gbs = k1_bytes(prec, lr) * sites / (k1_ms / max(k1_n, 1) * 1e-3) / 1e9
+    k2_gbs = k2_bytes(prec, lr) * sites / (k2_ms / max(k2_n, 1) * 1e-3) / 1e9
     k1_64 = sum(r.dslash_ms for r in r64) / max(sum(r.dslash_launches for r in r64), 1)
     k2_64 = sum(r.update_ms for r in r64) / max(sum(r.update_launches for r in r64), 1)
-    gbs64 = k1_bytes("double") * sites / (k1_64 * 1e-3) / 1e9
+    gbs64 = k1_bytes("double", lr64) * sites / (k1_64 * 1e-3) / 1e9
+    gbs64_k2 = k2_bytes("double", lr64) * sites / (k2_64 * 1e-3) / 1e9
     gflops = lambda ms: FLOPS_PER_SITE_M * sites / (ms * 1e-3) / 1e9
 
     line = {
@@ -394,7 +408,8 @@ def run_lmb(args):
                  "true_rel_residual": fp64_true},
         "speedup_mixed_vs_fp64": t_fp64 / t_mixed,
         "dslash": {
-            "fp64_k1_gbs": gbs64, "fp64_k1_gflops_M": gflops(k1_64),
+            "fp64_k1_gbs": gbs64, "fp64_k2_gbs": gbs64_k2,
+            "fp64_k1_gflops_M": gflops(k1_64), "link_reals": lr,
             "fp64_k1_ms": k1_64, "fp64_k2_ms": k2_64,
             f"{prec}_k1_gbs": k1_gbs, f"{prec}_k2_gbs": k2_gbs,
             f"{prec}_k1_ms": k1_ms / max(k1_n, 1),
@@ -426,6 +441,10 @@ def run_lmb(args):
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def res64_link_reals(results):
+    return results[-1].link_reals if results else 18
 
 
 class _Null:

@@ -82,6 +82,8 @@ typedef struct {
   double dslash_ms, update_ms; /* K1 (tmp = D p, |tmp|^2) and K2 (D'tmp + axpy) */
   int dslash_launches, update_launches;
   long long kernel_launches; /* liblmb200 kernels launched by this solve    */
+  int link_reals;            /* reals stored per link by the iterated stencil:
+                                18, or 12 for SU(3) links (third row rebuilt) */
 } lmb_cg_result;
 
 /* ---- context --------------------------------------------------------------
@@ -126,6 +128,48 @@ int lmb_wilson_apply(lmb_ctx *ctx, void *out, const void *in, double kappa,
 int lmb_wilson_clover_apply(lmb_ctx *ctx, void *out, const void *in,
                             double kappa, double csw, int dagger,
                             int precision, void *stream);
+
+/* mul!(out, StaggeredDiracOperator4D(U, mass), in) / adjoint
+ * (Operators/StaggeredDiracOperator.jl:165-198): thin links from
+ * lmb_links_upload(LMB_LINKS_THIN), 3 complex per site (NC x 1 fields). */
+int lmb_staggered_apply(lmb_ctx *ctx, void *out, const void *in, double mass,
+                        int dagger, int precision, void *stream);
+
+/* mul!(out, HISQDiracOperator4D(HISQLinks4D(X, L), mass; naik_epsilon), in)
+ * / adjoint and mul_cached_hisq! (Operators/HISQDiracOperator.jl:359-435,
+ * HISQFullSmearing.jl:457-485): fat and Naik links from
+ * lmb_links_upload(LMB_LINKS_FAT / LMB_LINKS_LONG). */
+int lmb_hisq_apply(lmb_ctx *ctx, void *out, const void *in, double mass,
+                   double naik_epsilon, int dagger, int precision,
+                   void *stream);
+
+/* HISQ smearing (FP64), on padded (3,3,...) link fields.
+ * lmb_hisq_fat7: Fat7 + Lepage with coefficients (c1, c3, c5, c7, cLepage):
+ *   hisq_fat7_level1! uses (1/8, 1/16, 1/64, 1/384, 0), hisq_fat7_level2!
+ *   (1 + eps/8, 1/16, 1/64, 1/384, -1/8) (Operators/HISQSmearing.jl:1112-1148,
+ *   1313-1379; factorised form :768-974).
+ * lmb_hisq_project_u3: W = V (V^+V)^{-1/2} (HISQFullSmearing.jl:100-128).
+ * lmb_hisq_naik: L_mu(x) = W_mu(x) W_mu(x+mu) W_mu(x+2mu)
+ *   (HISQFullSmearing.jl:136-195). */
+int lmb_hisq_fat7(lmb_ctx *ctx, const void *const U[4],
+                  const double coefficients[5], void *const V[4],
+                  void *stream);
+int lmb_hisq_project_u3(lmb_ctx *ctx, const void *const V[4],
+                        void *const W[4], void *stream);
+int lmb_hisq_naik(lmb_ctx *ctx, const void *const W[4], void *const L[4],
+                  void *stream);
+
+/* hisq_links_from_thin! (HISQFullSmearing.jl:261-338): level-1 Fat7, U(3)
+ * projection, level-2 Fat7 + Lepage, Naik.  The fat and Naik links become the
+ * context's LMB_LINKS_FAT / LMB_LINKS_LONG sets for lmb_hisq_apply and the
+ * HISQ CG, cached by thin-link pointer + epoch + naik_epsilon as
+ * HISQDiracCache4D / _ensure_hisq_cache_current! (HISQFullSmearing.jl:
+ * 340-441), so mul_cached_hisq! re-smears only when a link changes.  X and L
+ * (four padded fields each) receive copies when non-NULL. */
+int lmb_hisq_links_from_thin(lmb_ctx *ctx, const void *const U[4],
+                             const uint64_t epoch[4], double naik_epsilon,
+                             void *const X[4], void *const L[4],
+                             void *stream);
 
 /* CloverFieldStrength4D(U) components (12,13,14,23,24,34) written to six
  * padded (3,3,...) fields (Operators/WilsonDiracCloverOperator.jl:28-35,

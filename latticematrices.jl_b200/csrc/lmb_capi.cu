@@ -6,6 +6,7 @@
 
 #include "lmb_context.cuh"
 #include "lmb_random.cuh"
+#include "lmb_hisq_smear.cuh"
 
 using namespace lmb;
 
@@ -18,8 +19,34 @@ bool ctx_ok(lmb_ctx *ctx) { return ctx != nullptr; }
 // ---------------------------------------------------------------------------
 // link caches
 // ---------------------------------------------------------------------------
-int ensure_link_precision(lmb_ctx *ctx, LinkSet &ls, int prec, cudaStream_t st) {
+int ensure_link_precision(lmb_ctx *ctx, LinkSet &ls, int prec, cudaStream_t st, bool allow_recon = true) {
   const int64_t n = 36 * ctx->g.V;
+  const int64_t V = ctx->g.V;
+  if (allow_recon && ls.recon(prec)) {
+    double2 *d = nullptr;
+    float4 *f = nullptr;
+    int4 *h = nullptr;
+    if (prec == PREC_DOUBLE && ls.d12_version != ls.version) {
+      if (!ls.d12) LMB_CUDA(ctx, cudaMalloc(&ls.d12, sizeof(double2) * 24 * V));
+      d = ls.d12;
+      ls.d12_version = ls.version;
+    }
+    if (prec == PREC_SINGLE && ls.f12_version != ls.version) {
+      if (!ls.f12) LMB_CUDA(ctx, cudaMalloc(&ls.f12, sizeof(float4) * 12 * V));
+      f = ls.f12;
+      ls.f12_version = ls.version;
+    }
+    if (prec == PREC_HALF && ls.h12_version != ls.version) {
+      if (!ls.h12) LMB_CUDA(ctx, cudaMalloc(&ls.h12, sizeof(int4) * 6 * V));
+      h = ls.h12;
+      ls.h12_version = ls.version;
+    }
+    if (d || f || h) {
+      links_to_recon12_kernel<<<grid_for(V, 256), 256, 0, st>>>(d, f, h, ls.d, V);
+      LMB_CHECK_LAUNCH(ctx);
+    }
+    return LMB_OK;
+  }
   if (prec == PREC_SINGLE && ls.f_version != ls.version) {
     if (!ls.f) LMB_CUDA(ctx, cudaMalloc(&ls.f, sizeof(float2) * n));
     links_to_single_kernel<<<grid_for(n, 256), 256, 0, st>>>(ls.f, ls.d, n);
@@ -28,7 +55,7 @@ int ensure_link_precision(lmb_ctx *ctx, LinkSet &ls, int prec, cudaStream_t st) 
   }
   if (prec == PREC_HALF && ls.h_version != ls.version) {
     if (!ls.h) LMB_CUDA(ctx, cudaMalloc(&ls.h, sizeof(int) * n));
-    links_to_half_kernel<<<grid_for(n, 256), 256, 0, st>>>(ls.h, ls.d, n, ls.scale);
+    links_to_half_kernel<<<grid_for(n, 256), 256, 0, st>>>(ls.h, ls.d, n, pow2_exponent(ls.scale));
     LMB_CHECK_LAUNCH(ctx);
     ls.h_version = ls.version;
   }
@@ -49,10 +76,17 @@ float device_absmax(lmb_ctx *ctx, const double2 *p, int64_t n, cudaStream_t st, 
   return f;
 }
 
+template <int P> Gauge12<P> gauge12_view(const LinkSet &ls, int64_t V);
+template <> Gauge12<PREC_DOUBLE> gauge12_view<PREC_DOUBLE>(const LinkSet &ls, int64_t V) { return {ls.d12, V, 1.f}; }
+template <> Gauge12<PREC_SINGLE> gauge12_view<PREC_SINGLE>(const LinkSet &ls, int64_t V) { return {ls.f12, V, 1.f}; }
+template <> Gauge12<PREC_HALF> gauge12_view<PREC_HALF>(const LinkSet &ls, int64_t V) { return {ls.h12, V, 1.f}; }
+
 template <int P> Gauge<P> gauge_view(const LinkSet &ls, int64_t V);
 template <> Gauge<PREC_DOUBLE> gauge_view<PREC_DOUBLE>(const LinkSet &ls, int64_t V) { return {ls.d, V, ls.scale}; }
 template <> Gauge<PREC_SINGLE> gauge_view<PREC_SINGLE>(const LinkSet &ls, int64_t V) { return {ls.f, V, ls.scale}; }
-template <> Gauge<PREC_HALF> gauge_view<PREC_HALF>(const LinkSet &ls, int64_t V) { return {ls.h, V, ls.scale}; }
+template <> Gauge<PREC_HALF> gauge_view<PREC_HALF>(const LinkSet &ls, int64_t V) {
+  return {ls.h, V, base_of_exponent(pow2_exponent(ls.scale))};
+}
 
 // ---------------------------------------------------------------------------
 // clover cache
@@ -94,9 +128,11 @@ int ensure_clover(lmb_ctx *ctx, double coef, int prec, cudaStream_t st) {
   if (prec == PREC_HALF && cc.h_version != cc.d_version) {
     if (!cc.h) LMB_CUDA(ctx, cudaMalloc(&cc.h, sizeof(int4) * 8 * V));
     if (!cc.ht) LMB_CUDA(ctx, cudaMalloc(&cc.ht, sizeof(int2) * 2 * V));
-    cc.scale = device_absmax(ctx, cc.d, 36 * V, st, &rc);
+    const float amax = device_absmax(ctx, cc.d, 36 * V, st, &rc);
     if (rc) return rc;
-    clover_to_half_kernel<<<grid_for(V, 256), 256, 0, st>>>(cc.h, cc.ht, cc.d, V, cc.scale);
+    const int kexp = pow2_exponent(amax);
+    cc.scale = base_of_exponent(kexp);
+    clover_to_half_kernel<<<grid_for(V, 256), 256, 0, st>>>(cc.h, cc.ht, cc.d, V, kexp);
     LMB_CHECK_LAUNCH(ctx);
     cc.h_version = cc.d_version;
   }
@@ -118,12 +154,11 @@ template <> Clover<PREC_HALF> clover_view<PREC_HALF>(const CloverCache &cc, int6
 // ---------------------------------------------------------------------------
 // stencil launch
 // ---------------------------------------------------------------------------
-template <int PS, int PG, bool CLOVER, class Epi>
-int launch_wilson(lmb_ctx *ctx, const Field<PS, 12> &in, int dagger, double kappa, const Epi &epi,
-                  cudaStream_t st) {
+template <int PS, int PG, bool CLOVER, class G, class Epi>
+int launch_wilson_g(lmb_ctx *ctx, const Field<PS, 12> &in, const G &U, int dagger, double kappa, const Epi &epi,
+                    cudaStream_t st) {
   typedef typename Real<PS>::type R;
   const Geom &g = ctx->g;
-  const Gauge<PG> U = gauge_view<PG>(ctx->links[LMB_LINKS_THIN], g.V);
   const unsigned grid = grid_for(g.V, kDslashThreads);
   if constexpr (CLOVER) {
     const Clover<PG> A = clover_view<PG>(ctx->clover, g.V);
@@ -142,24 +177,91 @@ int launch_wilson(lmb_ctx *ctx, const Field<PS, 12> &in, int dagger, double kapp
   return LMB_OK;
 }
 
-template <int PS, class Epi>
-int launch_op(lmb_ctx *ctx, int op, const Field<PS, 12> &in, int dagger, double kappa, const Epi &epi,
-              cudaStream_t st) {
-  if (op == LMB_OP_WILSON_CLOVER) return launch_wilson<PS, PS, true>(ctx, in, dagger, kappa, epi, st);
-  return launch_wilson<PS, PS, false>(ctx, in, dagger, kappa, epi, st);
+template <int PS, int PG, bool CLOVER, class Epi>
+int launch_wilson(lmb_ctx *ctx, const Field<PS, 12> &in, int dagger, double kappa, const Epi &epi,
+                  cudaStream_t st) {
+  const LinkSet &ls = ctx->links[LMB_LINKS_THIN];
+  if (ls.recon(PG))
+    return launch_wilson_g<PS, PG, CLOVER>(ctx, in, gauge12_view<PG>(ls, ctx->g.V), dagger, kappa, epi, st);
+  return launch_wilson_g<PS, PG, CLOVER>(ctx, in, gauge_view<PG>(ls, ctx->g.V), dagger, kappa, epi, st);
 }
 
-int prepare_operator(lmb_ctx *ctx, int op, double kappa, double csw, int prec, cudaStream_t st) {
-  if (!ctx->geom_set) return fail(ctx, LMB_ERR_STATE, "lmb_set_geometry has not been called");
-  if (op != LMB_OP_WILSON && op != LMB_OP_WILSON_CLOVER)
-    return fail(ctx, LMB_ERR_UNSUPPORTED, "operator %d is not available in this build", op);
-  if (!ctx->links[LMB_LINKS_THIN].valid) return fail(ctx, LMB_ERR_STATE, "gauge links have not been uploaded");
+int check_prec(lmb_ctx *ctx, int prec) {
   if (prec < PREC_DOUBLE || prec > PREC_HALF) return fail(ctx, LMB_ERR_ARG, "unknown precision %d", prec);
-  int rc = ensure_link_precision(ctx, ctx->links[LMB_LINKS_THIN], prec, st);
-  if (rc) return rc;
-  if (op == LMB_OP_WILSON_CLOVER) return ensure_clover(ctx, -kappa * csw, prec, st);
   return LMB_OK;
 }
+
+// ---------------------------------------------------------------------------
+// operator policies: what to prepare and how to launch one stencil
+// ---------------------------------------------------------------------------
+struct WilsonPolicy {
+  static constexpr int NC = 12;
+  int op;
+  double kappa, csw;
+  int prepare(lmb_ctx *ctx, int prec, cudaStream_t st) const {
+    if (!ctx->geom_set) return fail(ctx, LMB_ERR_STATE, "lmb_set_geometry has not been called");
+    if (!ctx->links[LMB_LINKS_THIN].valid) return fail(ctx, LMB_ERR_STATE, "gauge links have not been uploaded");
+    int rc = check_prec(ctx, prec);
+    if (rc) return rc;
+    rc = ensure_link_precision(ctx, ctx->links[LMB_LINKS_THIN], prec, st);
+    if (rc) return rc;
+    if (op == LMB_OP_WILSON_CLOVER) return ensure_clover(ctx, -kappa * csw, prec, st);
+    return LMB_OK;
+  }
+  template <int P, class Epi>
+  int launch(lmb_ctx *ctx, const Field<P, 12> &in, int dagger, const Epi &epi, cudaStream_t st) const {
+    if (op == LMB_OP_WILSON_CLOVER) return launch_wilson<P, P, true>(ctx, in, dagger, kappa, epi, st);
+    return launch_wilson<P, P, false>(ctx, in, dagger, kappa, epi, st);
+  }
+  int link_reals(const lmb_ctx *ctx, int prec) const { return ctx->links[LMB_LINKS_THIN].recon(prec) ? 12 : 18; }
+};
+
+struct StaggeredPolicy {
+  static constexpr int NC = 3;
+  bool naik;  // HISQ: fat links X (LMB_LINKS_FAT) and Naik links L (LMB_LINKS_LONG)
+  double mass, eps;
+  int prepare(lmb_ctx *ctx, int prec, cudaStream_t st) const {
+    if (!ctx->geom_set) return fail(ctx, LMB_ERR_STATE, "lmb_set_geometry has not been called");
+    int rc = check_prec(ctx, prec);
+    if (rc) return rc;
+    if (naik) {
+      if (!ctx->links[LMB_LINKS_FAT].valid || !ctx->links[LMB_LINKS_LONG].valid)
+        return fail(ctx, LMB_ERR_STATE, "HISQ fat and long links have not been uploaded");
+      rc = ensure_link_precision(ctx, ctx->links[LMB_LINKS_FAT], prec, st, false);
+      if (rc) return rc;
+      return ensure_link_precision(ctx, ctx->links[LMB_LINKS_LONG], prec, st, false);
+    }
+    if (!ctx->links[LMB_LINKS_THIN].valid) return fail(ctx, LMB_ERR_STATE, "gauge links have not been uploaded");
+    return ensure_link_precision(ctx, ctx->links[LMB_LINKS_THIN], prec, st);
+  }
+  template <int P, class Epi>
+  int launch(lmb_ctx *ctx, const Field<P, 3> &in, int dagger, const Epi &epi, cudaStream_t st) const {
+    typedef typename Real<P>::type R;
+    const Geom &g = ctx->g;
+    const unsigned grid = grid_for(g.V, kStagThreads);
+    const R fc = (R)(dagger ? -0.5 : 0.5);
+    const R lc = (R)(dagger ? (1.0 + eps) / 48.0 : -(1.0 + eps) / 48.0);
+    if (naik) {
+      const Gauge<P> X = gauge_view<P>(ctx->links[LMB_LINKS_FAT], g.V);
+      const Gauge<P> Lk = gauge_view<P>(ctx->links[LMB_LINKS_LONG], g.V);
+      staggered_dslash_kernel<R, true><<<grid, kStagThreads, 0, st>>>(g, in, X, Lk, (R)mass, fc, lc, epi);
+    } else {
+      const LinkSet &ls = ctx->links[LMB_LINKS_THIN];
+      const NoLinks none{g.V};
+      if (ls.recon(P))
+        staggered_dslash_kernel<R, false><<<grid, kStagThreads, 0, st>>>(g, in, gauge12_view<P>(ls, g.V), none,
+                                                                          (R)mass, fc, lc, epi);
+      else
+        staggered_dslash_kernel<R, false><<<grid, kStagThreads, 0, st>>>(g, in, gauge_view<P>(ls, g.V), none,
+                                                                          (R)mass, fc, lc, epi);
+    }
+    LMB_CHECK_LAUNCH(ctx);
+    return LMB_OK;
+  }
+  int link_reals(const lmb_ctx *ctx, int prec) const {
+    return (!naik && ctx->links[LMB_LINKS_THIN].recon(prec)) ? 12 : 18;
+  }
+};
 
 template <int PS, int NC>
 int pack_in(lmb_ctx *ctx, Field<PS, NC> &f, const void *src, cudaStream_t st) {
@@ -183,32 +285,32 @@ int unpack_out(lmb_ctx *ctx, void *dst, const Field<PS, NC> &f, cudaStream_t st)
   return LMB_OK;
 }
 
-template <int PS>
-int apply_wilson_family(lmb_ctx *ctx, int op, void *out, const void *in, double kappa, int dagger,
-                        cudaStream_t st) {
-  Field<PS, 12> fin, fout;
+template <int PS, class Op>
+int apply_generic(lmb_ctx *ctx, const Op &op, void *out, const void *in, int dagger, cudaStream_t st) {
+  constexpr int NC = Op::NC;
+  Field<PS, NC> fin, fout;
   if (!make_field(ctx, "apply_in", fin) || !make_field(ctx, "apply_out", fout))
     return fail(ctx, LMB_ERR_CUDA, "out of device memory (apply workspaces)");
   int rc = pack_in(ctx, fin, in, st);
   if (rc) return rc;
-  EpiStore<PS> epi{fout, nullptr};
-  rc = launch_op<PS>(ctx, op, fin, dagger, kappa, epi, st);
+  EpiStore<PS, NC> epi{fout, nullptr};
+  rc = op.template launch<PS>(ctx, fin, dagger, epi, st);
   if (rc) return rc;
   return unpack_out(ctx, out, fout, st);
 }
 
-int apply_dispatch(lmb_ctx *ctx, int op, void *out, const void *in, double kappa, double csw, int dagger,
-                   int prec, void *stream) {
+template <class Op>
+int apply_dispatch(lmb_ctx *ctx, const Op &op, void *out, const void *in, int dagger, int prec, void *stream) {
   if (!ctx_ok(ctx)) return LMB_ERR_ARG;
   if (!out || !in) return fail(ctx, LMB_ERR_ARG, "null field pointer");
   if (out == in) return fail(ctx, LMB_ERR_ARG, "mul! requires distinct result and input fields");
   cudaStream_t st = as_stream(stream);
-  int rc = prepare_operator(ctx, op, kappa, csw, prec, st);
+  int rc = op.prepare(ctx, prec, st);
   if (rc) return rc;
   switch (prec) {
-    case PREC_DOUBLE: return apply_wilson_family<PREC_DOUBLE>(ctx, op, out, in, kappa, dagger, st);
-    case PREC_SINGLE: return apply_wilson_family<PREC_SINGLE>(ctx, op, out, in, kappa, dagger, st);
-    default: return apply_wilson_family<PREC_HALF>(ctx, op, out, in, kappa, dagger, st);
+    case PREC_DOUBLE: return apply_generic<PREC_DOUBLE>(ctx, op, out, in, dagger, st);
+    case PREC_SINGLE: return apply_generic<PREC_SINGLE>(ctx, op, out, in, dagger, st);
+    default: return apply_generic<PREC_HALF>(ctx, op, out, in, dagger, st);
   }
 }
 
@@ -236,37 +338,36 @@ int read_state(lmb_ctx *ctx, cudaStream_t st) {
 }
 
 // PS: precision of the iterated fields (DOUBLE = plain FP64 CG), PX: of x_low
-template <int PS, int PX>
-int cg_run(lmb_ctx *ctx, const lmb_cg_params *prm, void *x_pad, const void *b_pad, lmb_cg_result *res,
-           cudaStream_t st) {
+template <int PS, int PX, class Op>
+int cg_run(lmb_ctx *ctx, const lmb_cg_params *prm, const Op &op, void *x_pad, const void *b_pad,
+           lmb_cg_result *res, cudaStream_t st) {
   constexpr bool mixed = PS != PREC_DOUBLE;
+  constexpr int NC = Op::NC;
   const int64_t V = ctx->g.V;
-  const int op = prm->op;
-  const double kappa = prm->kappa;
   int rc;
   long long nl = 0;  // liblmb200 kernels launched by this solve
-  Field<PREC_DOUBLE, 12> b64, x64, r64, t64;
+  Field<PREC_DOUBLE, NC> b64, x64, r64, t64;
   if (!make_field(ctx, "cg_b", b64) || !make_field(ctx, "cg_x", x64) || !make_field(ctx, "cg_r", r64) ||
       !make_field(ctx, "cg_t", t64))
     return fail(ctx, LMB_ERR_CUDA, "out of device memory (CG FP64 fields)");
-  Field<PS, 12> p, rl, tl;
-  Field<PX, 12> xl;
+  Field<PS, NC> p, rl, tl;
+  Field<PX, NC> xl;
   if (!make_field(ctx, "cg_p", p)) return fail(ctx, LMB_ERR_CUDA, "out of device memory (CG p)");
   if constexpr (mixed) {
     if (!make_field(ctx, "cg_rl", rl) || !make_field(ctx, "cg_tl", tl) || !make_field(ctx, "cg_xl", xl))
       return fail(ctx, LMB_ERR_CUDA, "out of device memory (CG low-precision fields)");
   } else {
-    rl = *(Field<PS, 12> *)&r64;
-    tl = *(Field<PS, 12> *)&t64;
-    xl = *(Field<PX, 12> *)&x64;
+    rl = *(Field<PS, NC> *)&r64;
+    tl = *(Field<PS, NC> *)&t64;
+    xl = *(Field<PX, NC> *)&x64;
   }
   const unsigned dgrid = grid_for(V, kDslashThreads), bgrid = grid_for(V, kBlasThreads);
   if (!ensure_partials(ctx, dgrid > bgrid ? dgrid : bgrid, 1))
     return fail(ctx, LMB_ERR_CUDA, "out of device memory (reduction partials)");
-  rc = prepare_operator(ctx, op, kappa, prm->csw, PREC_DOUBLE, st);
+  rc = op.prepare(ctx, PREC_DOUBLE, st);
   if (rc) return rc;
   if (mixed) {
-    rc = prepare_operator(ctx, op, kappa, prm->csw, PS, st);
+    rc = op.prepare(ctx, PS, st);
     if (rc) return rc;
   }
 
@@ -282,25 +383,25 @@ int cg_run(lmb_ctx *ctx, const lmb_cg_params *prm, void *x_pad, const void *b_pa
   if (rc) return rc;
   nl += 2;
   if constexpr (mixed) {
-    LMB_CUDA(ctx, cudaMemsetAsync(xl.data, 0, Field<PX, 12>::bytes(V), st));
-    if (xl.norm) LMB_CUDA(ctx, cudaMemsetAsync(xl.norm, 0, Field<PX, 12>::norm_bytes(V), st));
+    LMB_CUDA(ctx, cudaMemsetAsync(xl.data, 0, Field<PX, NC>::bytes(V), st));
+    if (xl.norm) LMB_CUDA(ctx, cudaMemsetAsync(xl.norm, 0, Field<PX, NC>::norm_bytes(V), st));
   }
-  norm_b_kernel<12><<<bgrid, kBlasThreads, 0, st>>>(b64, ctx->st_dev, V, prm->rtol, prm->atol, ctx->partials,
+  norm_b_kernel<NC><<<bgrid, kBlasThreads, 0, st>>>(b64, ctx->st_dev, V, prm->rtol, prm->atol, ctx->partials,
                                                      ctx->counter);
   LMB_CHECK_LAUNCH(ctx);
   nl++;
   // r = b - D'D x (FP64)
   auto true_residual = [&](int mode) -> int {
-    EpiStore<PREC_DOUBLE> e1{t64, nullptr};
-    int r2 = launch_op<PREC_DOUBLE>(ctx, op, x64, 0, kappa, e1, st);
+    EpiStore<PREC_DOUBLE, NC> e1{t64, nullptr};
+    int r2 = op.template launch<PREC_DOUBLE>(ctx, x64, 0, e1, st);
     if (r2) return r2;
     nl += 2;
-    EpiTrueResidual<PS> e2{b64, r64, rl, mixed ? 1 : 0, mode, ctx->st_dev, ctx->partials, ctx->counter};
-    return launch_op<PREC_DOUBLE>(ctx, op, t64, 1, kappa, e2, st);
+    EpiTrueResidual<PS, NC> e2{b64, r64, rl, mixed ? 1 : 0, mode, ctx->st_dev, ctx->partials, ctx->counter};
+    return op.template launch<PREC_DOUBLE>(ctx, t64, 1, e2, st);
   };
   rc = true_residual(0);
   if (rc) return rc;
-  convert_kernel<PS, PS, 12><<<bgrid, kBlasThreads, 0, st>>>(p, rl, V);
+  convert_kernel<PS, PS, NC><<<bgrid, kBlasThreads, 0, st>>>(p, rl, V);
   LMB_CHECK_LAUNCH(ctx);
   nl++;
   rc = read_state(ctx, st);
@@ -317,23 +418,23 @@ int cg_run(lmb_ctx *ctx, const lmb_cg_params *prm, void *x_pad, const void *b_pa
   double k1_ms = 0, k2_ms = 0;
   int k1_n = 0, k2_n = 0;
 
-  EpiStoreNorm<PS> epi1{tl, ctx->st_dev, ctx->partials, ctx->counter};
-  EpiCGUpdate<PS, PX> epi2{p, rl, xl, ctx->st_dev, ctx->partials, ctx->counter};
+  EpiStoreNorm<PS, NC> epi1{tl, ctx->st_dev, ctx->partials, ctx->counter};
+  EpiCGUpdate<PS, PX, NC> epi2{p, rl, xl, ctx->st_dev, ctx->partials, ctx->counter};
   while (hs->status == ST_RUNNING) {
     const int it0 = hs->iter;
     for (int i = 0; i < k; i++) {
       if (prm->profile) cudaEventRecord(pool.ev[4 * i], st);
-      rc = launch_op<PS>(ctx, op, p, 0, kappa, epi1, st);
+      rc = op.template launch<PS>(ctx, p, 0, epi1, st);
       if (rc) return rc;
       nl++;
       if (prm->profile) cudaEventRecord(pool.ev[4 * i + 1], st);
-      rc = launch_op<PS>(ctx, op, tl, 1, kappa, epi2, st);
+      rc = op.template launch<PS>(ctx, tl, 1, epi2, st);
       if (rc) return rc;
       nl++;
       if (prm->profile) cudaEventRecord(pool.ev[4 * i + 2], st);
-      cg_p_update_kernel<PS, 12><<<bgrid, kBlasThreads, 0, st>>>(p, rl, ctx->st_dev, V);
+      cg_p_update_kernel<PS, NC><<<bgrid, kBlasThreads, 0, st>>>(p, rl, ctx->st_dev, V);
       LMB_CHECK_LAUNCH(ctx);
-  nl++;
+      nl++;
       if (prm->profile) cudaEventRecord(pool.ev[4 * i + 3], st);
     }
     rc = read_state(ctx, st);
@@ -352,24 +453,24 @@ int cg_run(lmb_ctx *ctx, const lmb_cg_params *prm, void *x_pad, const void *b_pa
     }
     if (hs->status == ST_RELIABLE) {
       if constexpr (mixed) {
-        fold_kernel<PX, 12><<<bgrid, kBlasThreads, 0, st>>>(x64, xl, V);
+        fold_kernel<PX, NC><<<bgrid, kBlasThreads, 0, st>>>(x64, xl, V);
         LMB_CHECK_LAUNCH(ctx);
-  nl++;
+        nl++;
         // resume: the true-residual kernel runs regardless of the pause
         rc = true_residual(1);
         if (rc) return rc;
-        cg_p_update_kernel<PS, 12><<<bgrid, kBlasThreads, 0, st>>>(p, rl, ctx->st_dev, V);
+        cg_p_update_kernel<PS, NC><<<bgrid, kBlasThreads, 0, st>>>(p, rl, ctx->st_dev, V);
         LMB_CHECK_LAUNCH(ctx);
-  nl++;
+        nl++;
         rc = read_state(ctx, st);
         if (rc) return rc;
       }
     }
   }
   if constexpr (mixed) {
-    fold_kernel<PX, 12><<<bgrid, kBlasThreads, 0, st>>>(x64, xl, V);
+    fold_kernel<PX, NC><<<bgrid, kBlasThreads, 0, st>>>(x64, xl, V);
     LMB_CHECK_LAUNCH(ctx);
-  nl++;
+    nl++;
   }
   const int status = hs->status;
   CGState final_state = *hs;
@@ -408,7 +509,19 @@ int cg_run(lmb_ctx *ctx, const lmb_cg_params *prm, void *x_pad, const void *b_pa
   res->dslash_launches = k1_n;
   res->update_launches = k2_n;
   res->kernel_launches = nl;
+  res->link_reals = op.link_reals(ctx, PS);
   return LMB_OK;
+}
+
+template <class Op>
+int cg_dispatch(lmb_ctx *ctx, const lmb_cg_params *prm, const Op &op, void *x, const void *b,
+                lmb_cg_result *res, cudaStream_t st) {
+  switch (prm->precision) {
+    case PREC_DOUBLE: return cg_run<PREC_DOUBLE, PREC_DOUBLE>(ctx, prm, op, x, b, res, st);
+    case PREC_SINGLE: return cg_run<PREC_SINGLE, PREC_SINGLE>(ctx, prm, op, x, b, res, st);
+    case PREC_HALF: return cg_run<PREC_HALF, PREC_SINGLE>(ctx, prm, op, x, b, res, st);
+    default: return fail(ctx, LMB_ERR_ARG, "unknown precision %d", prm->precision);
+  }
 }
 
 template <int NC>
@@ -438,6 +551,103 @@ __global__ void __launch_bounds__(256)
     out[0] = tot[0];
     out[1] = tot[1];
   }
+}
+
+// ---------------------------------------------------------------------------
+// HISQ smearing drivers (all FP64 on 36-plane link arrays)
+// ---------------------------------------------------------------------------
+int pack_links_to(lmb_ctx *ctx, double2 *dst, const void *const U[4], cudaStream_t st) {
+  const unsigned grid = grid_for(ctx->g.V, 256);
+  if (ctx->dtype == LMB_DTYPE_C128)
+    pack_links_kernel<double2><<<grid, 256, 0, st>>>(dst, (const double2 *)U[0], (const double2 *)U[1],
+                                                      (const double2 *)U[2], (const double2 *)U[3], ctx->g, ctx->pd);
+  else
+    pack_links_kernel<float2><<<grid, 256, 0, st>>>(dst, (const float2 *)U[0], (const float2 *)U[1],
+                                                     (const float2 *)U[2], (const float2 *)U[3], ctx->g, ctx->pd);
+  LMB_CHECK_LAUNCH(ctx);
+  return LMB_OK;
+}
+
+int unpack_links_from(lmb_ctx *ctx, void *const U[4], const double2 *src, cudaStream_t st) {
+  const unsigned grid = grid_for(ctx->g.V, 256);
+  if (ctx->dtype == LMB_DTYPE_C128)
+    unpack_links_kernel<double2><<<grid, 256, 0, st>>>((double2 *)U[0], (double2 *)U[1], (double2 *)U[2],
+                                                        (double2 *)U[3], src, ctx->g, ctx->pd);
+  else
+    unpack_links_kernel<float2><<<grid, 256, 0, st>>>((float2 *)U[0], (float2 *)U[1], (float2 *)U[2],
+                                                       (float2 *)U[3], src, ctx->g, ctx->pd);
+  LMB_CHECK_LAUNCH(ctx);
+  return LMB_OK;
+}
+
+// V = Fat7(U) with coefficients (c1, c3, c5, c7, cLepage)
+int fat7_planes(lmb_ctx *ctx, const double2 *U, double2 *V, const double *coef, cudaStream_t st) {
+  const int64_t n = ctx->g.V;
+  double2 *work = (double2 *)workspace(ctx, "smear_staples", sizeof(double2) * 54 * n);
+  if (!work) return fail(ctx, LMB_ERR_CUDA, "out of device memory (smearing staples)");
+  double2 *S3[3] = {work, work + 9 * n, work + 18 * n};
+  double2 *S5[3] = {work + 27 * n, work + 36 * n, work + 45 * n};
+  const unsigned grid = grid_for(n, kSmearThreads);
+  for (int mu = 0; mu < 4; mu++) {
+    int axes[3], k = 0;
+    for (int d = 0; d < 4; d++)
+      if (d != mu) axes[k++] = d;
+    const double2 *Umu = U + (size_t)mu * 9 * n;
+    double2 *Vmu = V + (size_t)mu * 9 * n;
+    for (int slot = 0; slot < 3; slot++)
+      staple_transport_kernel<<<grid, kSmearThreads, 0, st>>>(S3[slot], Umu, U, ctx->g, mu, axes[slot], 3, 0, 1.0);
+    for (int slot = 0; slot < 3; slot++) {
+      const int bs = slot == 0 ? 1 : 0, cs = slot == 2 ? 1 : 2;
+      staple_transport_kernel<<<grid, kSmearThreads, 0, st>>>(S5[slot], S3[cs], U, ctx->g, mu, axes[bs], 3, 0, 1.0);
+      staple_transport_kernel<<<grid, kSmearThreads, 0, st>>>(S5[slot], S3[bs], U, ctx->g, mu, axes[cs], 3, 1, 1.0);
+    }
+    fat7_combine_kernel<<<grid_for(9 * n, 256), 256, 0, st>>>(Vmu, Umu, S3[0], S3[1], S3[2], S5[0], S5[1], S5[2],
+                                                               n, coef[0], coef[1], coef[2]);
+    for (int slot = 0; slot < 3; slot++)
+      staple_transport_kernel<<<grid, kSmearThreads, 0, st>>>(Vmu, S5[slot], U, ctx->g, mu, axes[slot], 3, 1,
+                                                              coef[3]);
+  }
+  if (coef[4] != 0.0) lepage_kernel<<<grid_for(4 * n, kSmearThreads), kSmearThreads, 0, st>>>(V, U, ctx->g, coef[4]);
+  LMB_CHECK_LAUNCH(ctx);
+  return LMB_OK;
+}
+
+int project_u3_planes(lmb_ctx *ctx, const double2 *V, double2 *W, cudaStream_t st) {
+  u3_project_kernel<<<grid_for(4 * ctx->g.V, kSmearThreads), kSmearThreads, 0, st>>>(W, V, ctx->g.V);
+  LMB_CHECK_LAUNCH(ctx);
+  return LMB_OK;
+}
+
+int naik_planes(lmb_ctx *ctx, const double2 *W, double2 *L, cudaStream_t st) {
+  naik_kernel<<<grid_for(4 * ctx->g.V, kSmearThreads), kSmearThreads, 0, st>>>(L, W, ctx->g);
+  LMB_CHECK_LAUNCH(ctx);
+  return LMB_OK;
+}
+
+int check_links_arg(lmb_ctx *ctx, const void *const U[4], const char *what) {
+  if (!U) return fail(ctx, LMB_ERR_ARG, "null %s array", what);
+  for (int mu = 0; mu < 4; mu++)
+    if (!U[mu]) return fail(ctx, LMB_ERR_ARG, "%s[%d] is null", what, mu + 1);
+  return LMB_OK;
+}
+
+// install 36-plane links as a link set of the context (derived, not uploaded)
+int install_links(lmb_ctx *ctx, int which, const double2 *planes, cudaStream_t st) {
+  LinkSet &ls = ctx->links[which];
+  const int64_t V = ctx->g.V;
+  if (!ls.d) LMB_CUDA(ctx, cudaMalloc(&ls.d, sizeof(double2) * 36 * V));
+  LMB_CUDA(ctx, cudaMemcpyAsync(ls.d, planes, sizeof(double2) * 36 * V, cudaMemcpyDeviceToDevice, st));
+  int rc;
+  ls.scale = device_absmax(ctx, ls.d, 36 * V, st, &rc);
+  if (rc) return rc;
+  ls.su3_dev = 1.0;  // smeared links are not SU(3): never reconstruct
+  for (int mu = 0; mu < 4; mu++) {
+    ls.ptr[mu] = nullptr;
+    ls.epoch[mu] = 0;
+  }
+  ls.valid = true;
+  ls.version++;
+  return LMB_OK;
 }
 
 }  // namespace
@@ -472,6 +682,9 @@ void lmb_destroy(lmb_ctx *ctx) {
     cudaFree(ls.d);
     cudaFree(ls.f);
     cudaFree(ls.h);
+    cudaFree(ls.d12);
+    cudaFree(ls.f12);
+    cudaFree(ls.h12);
   }
   cudaFree(ctx->clover.F);
   cudaFree(ctx->clover.d);
@@ -528,8 +741,10 @@ int lmb_set_geometry(lmb_ctx *ctx, const int L[4], int nw, const double phase_re
   for (int mu = 0; mu < 4; mu++) ctx->pd.P[mu] = L[mu] + 2 * nw;
   ctx->dtype = dtype;
   ctx->geom_set = true;
-  if (changed)
+  if (changed) {
     for (auto &ls : ctx->links) ls.valid = false;
+    ctx->smear.valid = false;
+  }
   return LMB_OK;
 }
 
@@ -541,6 +756,7 @@ int lmb_links_upload(lmb_ctx *ctx, int which, const void *const U[4], const uint
   for (int mu = 0; mu < 4; mu++)
     if (!U[mu]) return fail(ctx, LMB_ERR_ARG, "gauge link U[%d] is null", mu + 1);
   LinkSet &ls = ctx->links[which];
+  if (which != LMB_LINKS_THIN) ctx->smear.valid = false;
   bool same = ls.valid;
   for (int mu = 0; mu < 4 && same; mu++)
     same = ls.ptr[mu] == U[mu] && epoch && ls.epoch[mu] == epoch[mu];
@@ -560,6 +776,19 @@ int lmb_links_upload(lmb_ctx *ctx, int which, const void *const U[4], const uint
   int rc;
   ls.scale = device_absmax(ctx, ls.d, 36 * V, st, &rc);
   if (rc) return rc;
+  {
+    unsigned *bits = (unsigned *)workspace(ctx, "su3dev", sizeof(unsigned));
+    if (!bits) return fail(ctx, LMB_ERR_CUDA, "out of device memory (su3 check)");
+    LMB_CUDA(ctx, cudaMemsetAsync(bits, 0, sizeof(unsigned), st));
+    su3_deviation_kernel<<<1184, 256, 0, st>>>(ls.d, V, bits);
+    LMB_CHECK_LAUNCH(ctx);
+    unsigned hb = 0;
+    LMB_CUDA(ctx, cudaMemcpyAsync(&hb, bits, sizeof hb, cudaMemcpyDeviceToHost, st));
+    LMB_CUDA(ctx, cudaStreamSynchronize(st));
+    float dev;
+    std::memcpy(&dev, &hb, sizeof dev);
+    ls.su3_dev = dev;
+  }
   for (int mu = 0; mu < 4; mu++) {
     ls.ptr[mu] = U[mu];
     ls.epoch[mu] = epoch ? epoch[mu] : 0;
@@ -571,12 +800,25 @@ int lmb_links_upload(lmb_ctx *ctx, int which, const void *const U[4], const uint
 
 int lmb_wilson_apply(lmb_ctx *ctx, void *out, const void *in, double kappa, int dagger, int precision,
                      void *stream) {
-  return apply_dispatch(ctx, LMB_OP_WILSON, out, in, kappa, 0.0, dagger, precision, stream);
+  return apply_dispatch(ctx, WilsonPolicy{LMB_OP_WILSON, kappa, 0.0}, out, in, dagger, precision, stream);
 }
 
 int lmb_wilson_clover_apply(lmb_ctx *ctx, void *out, const void *in, double kappa, double csw, int dagger,
                             int precision, void *stream) {
-  return apply_dispatch(ctx, LMB_OP_WILSON_CLOVER, out, in, kappa, csw, dagger, precision, stream);
+  return apply_dispatch(ctx, WilsonPolicy{LMB_OP_WILSON_CLOVER, kappa, csw}, out, in, dagger, precision, stream);
+}
+
+int lmb_staggered_apply(lmb_ctx *ctx, void *out, const void *in, double mass, int dagger, int precision,
+                        void *stream) {
+  if (ctx && !std::isfinite(mass)) return fail(ctx, LMB_ERR_ARG, "mass must be finite");
+  return apply_dispatch(ctx, StaggeredPolicy{false, mass, 0.0}, out, in, dagger, precision, stream);
+}
+
+int lmb_hisq_apply(lmb_ctx *ctx, void *out, const void *in, double mass, double naik_epsilon, int dagger,
+                   int precision, void *stream) {
+  if (ctx && !std::isfinite(mass)) return fail(ctx, LMB_ERR_ARG, "mass must be finite");
+  if (ctx && !std::isfinite(naik_epsilon)) return fail(ctx, LMB_ERR_ARG, "naik_epsilon must be finite");
+  return apply_dispatch(ctx, StaggeredPolicy{true, mass, naik_epsilon}, out, in, dagger, precision, stream);
 }
 
 int lmb_clover_field_strength(lmb_ctx *ctx, void *const F[6], void *stream) {
@@ -612,11 +854,17 @@ int lmb_cg_ddagd(lmb_ctx *ctx, const lmb_cg_params *prm, void *x, const void *b,
     return fail(ctx, LMB_ERR_ARG, "reliable-update delta must lie in (0, 1)");
   std::memset(res, 0, sizeof *res);
   cudaStream_t st = as_stream(stream);
-  switch (prm->precision) {
-    case PREC_DOUBLE: return cg_run<PREC_DOUBLE, PREC_DOUBLE>(ctx, prm, x, b, res, st);
-    case PREC_SINGLE: return cg_run<PREC_SINGLE, PREC_SINGLE>(ctx, prm, x, b, res, st);
-    case PREC_HALF: return cg_run<PREC_HALF, PREC_SINGLE>(ctx, prm, x, b, res, st);
-    default: return fail(ctx, LMB_ERR_ARG, "unknown precision %d", prm->precision);
+  switch (prm->op) {
+    case LMB_OP_WILSON:
+    case LMB_OP_WILSON_CLOVER:
+      return cg_dispatch(ctx, prm, WilsonPolicy{prm->op, prm->kappa, prm->csw}, x, b, res, st);
+    case LMB_OP_STAGGERED:
+      if (!std::isfinite(prm->mass)) return fail(ctx, LMB_ERR_ARG, "mass must be finite");
+      return cg_dispatch(ctx, prm, StaggeredPolicy{false, prm->mass, 0.0}, x, b, res, st);
+    case LMB_OP_HISQ:
+      if (!std::isfinite(prm->mass)) return fail(ctx, LMB_ERR_ARG, "mass must be finite");
+      return cg_dispatch(ctx, prm, StaggeredPolicy{true, prm->mass, prm->naik_epsilon}, x, b, res, st);
+    default: return fail(ctx, LMB_ERR_ARG, "unknown operator %d", prm->op);
   }
 }
 
@@ -676,6 +924,104 @@ int lmb_gaussian_field(lmb_ctx *ctx, void *out, int ncomp, uint64_t seed, void *
   else
     gaussian_field_kernel<float2><<<grid, 256, 0, st>>>((float2 *)out, ncomp, ctx->g, ctx->pd, seed);
   LMB_CHECK_LAUNCH(ctx);
+  return LMB_OK;
+}
+
+
+int lmb_hisq_fat7(lmb_ctx *ctx, const void *const U[4], const double coefficients[5], void *const V[4],
+                  void *stream) {
+  if (!ctx_ok(ctx)) return LMB_ERR_ARG;
+  if (!ctx->geom_set) return fail(ctx, LMB_ERR_STATE, "lmb_set_geometry has not been called");
+  int rc = check_links_arg(ctx, U, "input link");
+  if (rc) return rc;
+  if ((rc = check_links_arg(ctx, (const void *const *)V, "output link"))) return rc;
+  if (!coefficients) return fail(ctx, LMB_ERR_ARG, "null coefficients");
+  cudaStream_t st = as_stream(stream);
+  const int64_t n = ctx->g.V;
+  double2 *in = (double2 *)workspace(ctx, "smear_in", sizeof(double2) * 36 * n);
+  double2 *out = (double2 *)workspace(ctx, "smear_out", sizeof(double2) * 36 * n);
+  if (!in || !out) return fail(ctx, LMB_ERR_CUDA, "out of device memory (smearing)");
+  if ((rc = pack_links_to(ctx, in, U, st))) return rc;
+  if ((rc = fat7_planes(ctx, in, out, coefficients, st))) return rc;
+  return unpack_links_from(ctx, V, out, st);
+}
+
+int lmb_hisq_project_u3(lmb_ctx *ctx, const void *const V[4], void *const W[4], void *stream) {
+  if (!ctx_ok(ctx)) return LMB_ERR_ARG;
+  if (!ctx->geom_set) return fail(ctx, LMB_ERR_STATE, "lmb_set_geometry has not been called");
+  int rc = check_links_arg(ctx, V, "input link");
+  if (rc) return rc;
+  if ((rc = check_links_arg(ctx, (const void *const *)W, "output link"))) return rc;
+  cudaStream_t st = as_stream(stream);
+  const int64_t n = ctx->g.V;
+  double2 *in = (double2 *)workspace(ctx, "smear_in", sizeof(double2) * 36 * n);
+  double2 *out = (double2 *)workspace(ctx, "smear_out", sizeof(double2) * 36 * n);
+  if (!in || !out) return fail(ctx, LMB_ERR_CUDA, "out of device memory (smearing)");
+  if ((rc = pack_links_to(ctx, in, V, st))) return rc;
+  if ((rc = project_u3_planes(ctx, in, out, st))) return rc;
+  return unpack_links_from(ctx, W, out, st);
+}
+
+int lmb_hisq_naik(lmb_ctx *ctx, const void *const W[4], void *const L[4], void *stream) {
+  if (!ctx_ok(ctx)) return LMB_ERR_ARG;
+  if (!ctx->geom_set) return fail(ctx, LMB_ERR_STATE, "lmb_set_geometry has not been called");
+  int rc = check_links_arg(ctx, W, "input link");
+  if (rc) return rc;
+  if ((rc = check_links_arg(ctx, (const void *const *)L, "output link"))) return rc;
+  cudaStream_t st = as_stream(stream);
+  const int64_t n = ctx->g.V;
+  double2 *in = (double2 *)workspace(ctx, "smear_in", sizeof(double2) * 36 * n);
+  double2 *out = (double2 *)workspace(ctx, "smear_out", sizeof(double2) * 36 * n);
+  if (!in || !out) return fail(ctx, LMB_ERR_CUDA, "out of device memory (smearing)");
+  if ((rc = pack_links_to(ctx, in, W, st))) return rc;
+  if ((rc = naik_planes(ctx, in, out, st))) return rc;
+  return unpack_links_from(ctx, L, out, st);
+}
+
+int lmb_hisq_links_from_thin(lmb_ctx *ctx, const void *const U[4], const uint64_t epoch[4], double naik_epsilon,
+                             void *const X[4], void *const L[4], void *stream) {
+  if (!ctx_ok(ctx)) return LMB_ERR_ARG;
+  if (!ctx->geom_set) return fail(ctx, LMB_ERR_STATE, "lmb_set_geometry has not been called");
+  int rc = check_links_arg(ctx, U, "thin link");
+  if (rc) return rc;
+  if (!std::isfinite(naik_epsilon)) return fail(ctx, LMB_ERR_ARG, "naik_epsilon must be finite");
+  cudaStream_t st = as_stream(stream);
+  lmb_smear_key &key = ctx->smear;
+  bool same = key.valid && key.naik_epsilon == naik_epsilon && ctx->links[LMB_LINKS_FAT].valid &&
+              ctx->links[LMB_LINKS_LONG].valid && epoch;
+  for (int mu = 0; mu < 4 && same; mu++) same = key.ptr[mu] == U[mu] && key.epoch[mu] == epoch[mu];
+  const int64_t n = ctx->g.V;
+  if (!same) {
+    double2 *thin = (double2 *)workspace(ctx, "smear_thin", sizeof(double2) * 36 * n);
+    double2 *lvl1 = (double2 *)workspace(ctx, "smear_lvl1", sizeof(double2) * 36 * n);
+    double2 *w = (double2 *)workspace(ctx, "smear_w", sizeof(double2) * 36 * n);
+    double2 *xo = (double2 *)workspace(ctx, "smear_out", sizeof(double2) * 36 * n);
+    if (!thin || !lvl1 || !w || !xo) return fail(ctx, LMB_ERR_CUDA, "out of device memory (smearing)");
+    // hisq_links_from_thin! (HISQFullSmearing.jl:284-293)
+    const double c_level1[5] = {1.0 / 8, 1.0 / 16, 1.0 / 64, 1.0 / 384, 0.0};
+    const double c_level2[5] = {1.0 + naik_epsilon / 8, 1.0 / 16, 1.0 / 64, 1.0 / 384, -1.0 / 8};
+    if ((rc = pack_links_to(ctx, thin, U, st))) return rc;
+    if ((rc = fat7_planes(ctx, thin, lvl1, c_level1, st))) return rc;
+    if ((rc = project_u3_planes(ctx, lvl1, w, st))) return rc;
+    if ((rc = fat7_planes(ctx, w, xo, c_level2, st))) return rc;
+    if ((rc = install_links(ctx, LMB_LINKS_FAT, xo, st))) return rc;
+    if ((rc = naik_planes(ctx, w, xo, st))) return rc;
+    if ((rc = install_links(ctx, LMB_LINKS_LONG, xo, st))) return rc;
+    for (int mu = 0; mu < 4; mu++) {
+      key.ptr[mu] = U[mu];
+      key.epoch[mu] = epoch ? epoch[mu] : 0;
+    }
+    key.naik_epsilon = naik_epsilon;
+    key.valid = epoch != nullptr;
+  }
+  if (X) {
+    if ((rc = check_links_arg(ctx, (const void *const *)X, "fat link"))) return rc;
+    if ((rc = unpack_links_from(ctx, X, ctx->links[LMB_LINKS_FAT].d, st))) return rc;
+  }
+  if (L) {
+    if ((rc = check_links_arg(ctx, (const void *const *)L, "long link"))) return rc;
+    if ((rc = unpack_links_from(ctx, L, ctx->links[LMB_LINKS_LONG].d, st))) return rc;
+  }
   return LMB_OK;
 }
 

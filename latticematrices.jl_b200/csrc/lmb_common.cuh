@@ -57,6 +57,7 @@ template <typename R> LMB_HD Cx<R> cfma_conj(Cx<R> a, Cx<R> b, Cx<R> acc) {
 }
 template <typename R> LMB_HD R norm2(Cx<R> a) { return a.re * a.re + a.im * a.im; }
 
+
 // ---------------------------------------------------------------------------
 // geometry (single rank: periodic wrap with the fermion boundary phase)
 // ---------------------------------------------------------------------------
@@ -95,7 +96,6 @@ LMB_D int bwd_site(const Geom &g, int s, const int c[4], int mu, int d, int *wra
 // ---------------------------------------------------------------------------
 // storage traits
 // ---------------------------------------------------------------------------
-constexpr float kInt16Scale = 32767.0f;
 
 template <int P> struct Real { typedef float type; };
 template <> struct Real<PREC_DOUBLE> { typedef double type; };
@@ -154,50 +154,108 @@ template <int NCOMP> struct Field<PREC_SINGLE, NCOMP> {
   }
 };
 
+// three-component (staggered) FP32 field: three float2 planes, no padding
+template <> struct Field<PREC_SINGLE, 3> {
+  float2 *data;
+  float *norm;
+  int64_t V;
+  static constexpr int kPlanes = 3;
+  static size_t bytes(int64_t V) { return sizeof(float2) * 3 * V; }
+  static size_t norm_bytes(int64_t) { return 0; }
+  template <typename R> LMB_D void load(int64_t s, Cx<R> *v) const {
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const float2 t = __ldg(data + k * V + s);
+      v[k] = Cx<R>((R)t.x, (R)t.y);
+    }
+  }
+  template <typename R> LMB_D void store(int64_t s, const Cx<R> *v) const {
+#pragma unroll
+    for (int k = 0; k < 3; k++) data[k * V + s] = make_float2((float)v[k].re, (float)v[k].im);
+  }
+};
+
 LMB_D short f2s(float x) { return (short)__float2int_rn(x); }
+
+// int16 storage.  Every int16 group (a site's spinor, the links, the clover
+// blocks) carries a power-of-two scale 2^k with all |values| <= 2^k; a value
+// v is stored as u = q + 32768 with q = rint(v 2^-k 32768) in [-32767, 32767].
+// Decoding needs no integer conversion: with base = 2^(8+k), the float whose
+// exponent is base's and whose low 16 mantissa bits are u equals
+// base (1 + u 2^-23); subtracting base (1 + 2^-8) leaves q 2^(k-15) = v
+// exactly.  One byte permute builds each float, one packed FADD2 finishes a
+// complex pair.
+struct Dec16 {
+  unsigned y;  // high 16 bits of base (exponent field)
+  float c;     // base (1 + 2^-8)
+};
+LMB_D Dec16 dec16_of_base(float base) {
+  Dec16 d;
+  d.y = __float_as_uint(base) >> 16;
+  d.c = base * 1.00390625f;
+  return d;
+}
+LMB_D float2 dec_pair(int w, const Dec16 &d) {
+  const float lo = __uint_as_float(__byte_perm((unsigned)w, d.y, 0x5410u));
+  const float hi = __uint_as_float(__byte_perm((unsigned)w, d.y, 0x5432u));
+  return __fadd2_rn(make_float2(lo, hi), make_float2(-d.c, -d.c));
+}
+// scale exponent k for a maximum magnitude m (|v| <= m <= 2^k), and base
+LMB_HD int pow2_exponent(float m) {
+  if (!(m > 0.f)) return 0;
+  int e;
+  frexpf(m, &e);  // m = f 2^e, 0.5 <= f < 1, so m < 2^e
+  if (e < -130) e = -130;
+  if (e > 110) e = 110;
+  return e;
+}
+LMB_HD float base_of_exponent(int k) { return ldexpf(1.0f, 8 + k); }
+// encode a complex pair already scaled to [-32768, 32768]: clamp to
+// +-32767 and add 2^23 + 32768, so that the float's low 16 mantissa bits are
+// u = rint(q) + 32768; one byte permute packs the two halves (no F2I)
+LMB_D int enc_pair(float a, float b) {
+  const float fa = fminf(fmaxf(a, -32767.f), 32767.f) + 8421376.0f;
+  const float fb = fminf(fmaxf(b, -32767.f), 32767.f) + 8421376.0f;
+  return (int)__byte_perm(__float_as_uint(fa), __float_as_uint(fb), 0x5410u);
+}
 
 template <int NCOMP> struct Field<PREC_HALF, NCOMP> {
   int4 *data;
-  float *norm;
+  float *norm;  // per-site base 2^(8+k)
   int64_t V;
   static constexpr int kPlanes = (NCOMP + 3) / 4;
   static size_t bytes(int64_t V) { return sizeof(int4) * kPlanes * V; }
   static size_t norm_bytes(int64_t V) { return sizeof(float) * V; }
   template <typename R> LMB_D void load(int64_t s, Cx<R> *v) const {
-    const float scale = __ldg(norm + s) * (1.0f / kInt16Scale);
+    const Dec16 d = dec16_of_base(__ldg(norm + s));
 #pragma unroll
     for (int k = 0; k < kPlanes; k++) {
       int4 t = __ldg(data + k * V + s);
       const int w[4] = {t.x, t.y, t.z, t.w};
 #pragma unroll
-      for (int j = 0; j < 4; j++) {
+      for (int j = 0; j < 4; j++)
         if (4 * k + j < NCOMP) {
-          short lo = (short)(w[j] & 0xffff), hi = (short)(w[j] >> 16);
-          v[4 * k + j] = Cx<R>((R)((float)lo * scale), (R)((float)hi * scale));
+          const float2 f = dec_pair(w[j], d);
+          v[4 * k + j] = Cx<R>((R)f.x, (R)f.y);
         }
-      }
     }
   }
   template <typename R> LMB_D void store(int64_t s, const Cx<R> *v) const {
     float m = 0.f;
 #pragma unroll
     for (int k = 0; k < NCOMP; k++) m = fmaxf(m, fmaxf(fabsf((float)v[k].re), fabsf((float)v[k].im)));
-    const float inv = m > 0.f ? kInt16Scale / m : 0.f;
+    const int e = pow2_exponent(m);
+    const float inv = ldexpf(32768.0f, -e);
 #pragma unroll
     for (int k = 0; k < kPlanes; k++) {
       int w[4];
 #pragma unroll
-      for (int j = 0; j < 4; j++) {
-        if (4 * k + j < NCOMP) {
-          short lo = f2s((float)v[4 * k + j].re * inv), hi = f2s((float)v[4 * k + j].im * inv);
-          w[j] = ((int)(unsigned short)lo) | ((int)hi << 16);
-        } else {
-          w[j] = 0;
-        }
-      }
+      for (int j = 0; j < 4; j++)
+        w[j] = (4 * k + j < NCOMP) ? enc_pair((float)v[4 * k + j].re * inv, (float)v[4 * k + j].im * inv)
+                                   : enc_pair(0.f, 0.f);
       data[k * V + s] = make_int4(w[0], w[1], w[2], w[3]);
     }
-    norm[s] = m;
+    norm[s] = base_of_exponent(e);
   }
 };
 
@@ -234,15 +292,78 @@ template <> struct Gauge<PREC_SINGLE> {
 template <> struct Gauge<PREC_HALF> {
   const int *data;  // packed (re, im) int16 pairs
   int64_t V;
-  float scale;
+  float scale;      // base 2^(8+k) of the global power-of-two scale
   static size_t bytes(int64_t V) { return sizeof(int) * 36 * V; }
   template <typename R> LMB_D void load(int mu, int64_t s, Cx<R> *u) const {
-    const float f = scale * (1.0f / kInt16Scale);
+    const Dec16 d = dec16_of_base(scale);
 #pragma unroll
     for (int k = 0; k < 9; k++) {
-      int w = __ldg(data + (mu * 9 + k) * V + s);
-      u[k] = Cx<R>((R)((float)(short)(w & 0xffff) * f), (R)((float)(short)(w >> 16) * f));
+      const float2 f = dec_pair(__ldg(data + (mu * 9 + k) * V + s), d);
+      u[k] = Cx<R>((R)f.x, (R)f.y);
     }
+  }
+};
+
+// third row of an SU(3) matrix from the first two: row2 = conj(row0 x row1)
+// (the reconstruction of kernel_normalize_NC3!, linearalgebra_D.jl:2371-2424);
+// u column-major u[r + 3c]
+template <typename R>
+LMB_D void su3_third_row(Cx<R> *u) {
+  u[2] = conj(u[3] * u[7] - u[6] * u[4]);
+  u[5] = conj(u[6] * u[1] - u[0] * u[7]);
+  u[8] = conj(u[0] * u[4] - u[3] * u[1]);
+}
+
+// Links known to be SU(3): only rows 0 and 1 are stored (12 reals), entry
+// e = 3 r + c of direction mu.
+//  double: 24 double2 planes (mu*6 + e)
+//  single: 12 float4 planes (mu*3 + k), float4 k = entries 2k, 2k+1
+//  half  : 6 int4 planes; complex q = mu*6 + e sits in plane q/4, lane q%4;
+//          int16 values scaled by 1 (|U_ij| <= 1)
+template <int P> struct Gauge12;
+template <> struct Gauge12<PREC_DOUBLE> {
+  const double2 *data;
+  int64_t V;
+  float scale;
+  template <typename R> LMB_D void load(int mu, int64_t s, Cx<R> *u) const {
+#pragma unroll
+    for (int e = 0; e < 6; e++) {
+      const double2 t = __ldg(data + (mu * 6 + e) * V + s);
+      u[(e / 3) + 3 * (e % 3)] = Cx<R>((R)t.x, (R)t.y);
+    }
+    su3_third_row(u);
+  }
+};
+template <> struct Gauge12<PREC_SINGLE> {
+  const float4 *data;
+  int64_t V;
+  float scale;
+  template <typename R> LMB_D void load(int mu, int64_t s, Cx<R> *u) const {
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const float4 t = __ldg(data + (mu * 3 + k) * V + s);
+      const int e0 = 2 * k, e1 = 2 * k + 1;
+      u[(e0 / 3) + 3 * (e0 % 3)] = Cx<R>((R)t.x, (R)t.y);
+      u[(e1 / 3) + 3 * (e1 % 3)] = Cx<R>((R)t.z, (R)t.w);
+    }
+    su3_third_row(u);
+  }
+};
+template <> struct Gauge12<PREC_HALF> {
+  const int4 *data;
+  int64_t V;
+  float scale;  // unused: |U_ij| <= 1, scale exponent 0
+  template <typename R> LMB_D void load(int mu, int64_t s, Cx<R> *u) const {
+    const int q0 = mu * 6, p0 = q0 >> 2, lane0 = q0 & 3;
+    const int4 a = __ldg(data + p0 * V + s), b = __ldg(data + (p0 + 1) * V + s);
+    const int w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    const Dec16 d{0x4380u, 257.0f};  // base 2^8
+#pragma unroll
+    for (int e = 0; e < 6; e++) {
+      const float2 f = dec_pair(w[lane0 + e], d);
+      u[(e / 3) + 3 * (e % 3)] = Cx<R>((R)f.x, (R)f.y);
+    }
+    su3_third_row(u);
   }
 };
 
@@ -287,25 +408,27 @@ template <> struct Clover<PREC_HALF> {
   const int4 *data;  // 8 planes: block*4 + k
   const int2 *tail;  // 2 planes: block
   int64_t V;
-  float scale;
+  float scale;       // base 2^(8+k) of the global power-of-two scale
   static size_t bytes(int64_t V) { return (sizeof(int4) * 8 + sizeof(int2) * 2) * V; }
   template <typename R> LMB_D void load(int blk, int64_t s, R *a) const {
-    const float f = scale * (1.0f / kInt16Scale);
+    const Dec16 d = dec16_of_base(scale);
 #pragma unroll
     for (int k = 0; k < 4; k++) {
       int4 t = __ldg(data + (blk * 4 + k) * V + s);
       const int w[4] = {t.x, t.y, t.z, t.w};
 #pragma unroll
       for (int j = 0; j < 4; j++) {
-        a[8 * k + 2 * j] = (R)((float)(short)(w[j] & 0xffff) * f);
-        a[8 * k + 2 * j + 1] = (R)((float)(short)(w[j] >> 16) * f);
+        const float2 f = dec_pair(w[j], d);
+        a[8 * k + 2 * j] = (R)f.x;
+        a[8 * k + 2 * j + 1] = (R)f.y;
       }
     }
     int2 t = __ldg(tail + blk * V + s);
-    a[32] = (R)((float)(short)(t.x & 0xffff) * f);
-    a[33] = (R)((float)(short)(t.x >> 16) * f);
-    a[34] = (R)((float)(short)(t.y & 0xffff) * f);
-    a[35] = (R)((float)(short)(t.y >> 16) * f);
+    const float2 f0 = dec_pair(t.x, d), f1 = dec_pair(t.y, d);
+    a[32] = (R)f0.x;
+    a[33] = (R)f0.y;
+    a[34] = (R)f1.x;
+    a[35] = (R)f1.y;
   }
 };
 

@@ -24,6 +24,14 @@ struct LinkSet {
   int *h = nullptr;
   float scale = 1.f;     // max |element| (for int16)
   uint64_t f_version = ~0ull, h_version = ~0ull;
+  // SU(3) links store two rows (reconstruct-12); chosen per precision by the
+  // measured deviation max(|U U^+ - 1|, |det U - 1|) at upload
+  double su3_dev = 1.0;
+  double2 *d12 = nullptr;
+  float4 *f12 = nullptr;
+  int4 *h12 = nullptr;
+  uint64_t d12_version = ~0ull, f12_version = ~0ull, h12_version = ~0ull;
+  bool recon(int prec) const { return prec == PREC_DOUBLE ? su3_dev <= 1e-14 : su3_dev <= 1e-6; }
 };
 
 struct CloverCache {
@@ -43,8 +51,16 @@ struct CloverCache {
 
 }  // namespace lmb
 
+struct lmb_smear_key {
+  const void *ptr[4] = {nullptr, nullptr, nullptr, nullptr};
+  uint64_t epoch[4] = {0, 0, 0, 0};
+  double naik_epsilon = 0.0;
+  bool valid = false;
+};
+
 struct lmb_ctx {
   int device = 0;
+  lmb_smear_key smear;  // thin links the HISQ fat/long link sets were built from
   bool geom_set = false;
   lmb::Geom g{};
   lmb::Padded pd{};

@@ -83,14 +83,67 @@ __global__ void __launch_bounds__(256)
   dst[i] = make_float2((float)t.x, (float)t.y);
 }
 
+// k = scale exponent (|values| <= 2^k)
 __global__ void __launch_bounds__(256)
-    links_to_half_kernel(int *dst, const double2 *src, int64_t n, float scale) {
+    links_to_half_kernel(int *dst, const double2 *src, int64_t n, int k) {
   const int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x;
   if (i >= n) return;
   const double2 t = src[i];
-  const float inv = scale > 0.f ? kInt16Scale / scale : 0.f;
-  const short lo = f2s((float)t.x * inv), hi = f2s((float)t.y * inv);
-  dst[i] = ((int)(unsigned short)lo) | ((int)hi << 16);
+  const float inv = ldexpf(32768.0f, -k);
+  dst[i] = enc_pair((float)t.x * inv, (float)t.y * inv);
+}
+
+// 36 double2 link planes (mu*9 + r + 3c) -> rows 0, 1 only (SU(3) links)
+__global__ void __launch_bounds__(256)
+    links_to_recon12_kernel(double2 *d12, float4 *f12, int4 *h12, const double2 *src, int64_t V) {
+  const int64_t s = (int64_t)blockIdx.x * 256 + threadIdx.x;
+  if (s >= V) return;
+  double2 e[24];  // q = mu*6 + 3r + c
+  for (int mu = 0; mu < 4; mu++)
+    for (int r = 0; r < 2; r++)
+      for (int c = 0; c < 3; c++) e[mu * 6 + 3 * r + c] = src[(mu * 9 + r + 3 * c) * V + s];
+  if (d12)
+    for (int q = 0; q < 24; q++) d12[q * V + s] = e[q];
+  if (f12)
+    for (int k = 0; k < 12; k++)
+      f12[k * V + s] = make_float4((float)e[2 * k].x, (float)e[2 * k].y, (float)e[2 * k + 1].x, (float)e[2 * k + 1].y);
+  if (h12)
+    for (int k = 0; k < 6; k++) {
+      int w[4];
+      for (int j = 0; j < 4; j++)
+        w[j] = enc_pair((float)e[4 * k + j].x * 32768.0f, (float)e[4 * k + j].y * 32768.0f);
+      h12[k * V + s] = make_int4(w[0], w[1], w[2], w[3]);
+    }
+}
+
+// max over links of |U U^+ - 1| and |det U - 1| (float bits, atomicMax)
+__global__ void __launch_bounds__(256)
+    su3_deviation_kernel(const double2 *U, int64_t V, unsigned *out_bits) {
+  float m = 0.f;
+  for (int64_t t = (int64_t)blockIdx.x * 256 + threadIdx.x; t < 4 * V; t += (int64_t)gridDim.x * 256) {
+    const int mu = (int)(t / V);
+    const int64_t s = t - mu * V;
+    Cx<double> u[9];
+    for (int k = 0; k < 9; k++) {
+      const double2 x = U[(mu * 9 + k) * V + s];
+      u[k] = Cx<double>(x.x, x.y);
+    }
+    double dev = 0;
+    for (int r = 0; r < 3; r++)
+      for (int c = 0; c < 3; c++) {
+        Cx<double> v(0, 0);
+        for (int k = 0; k < 3; k++) v = cfma_conj(u[c + 3 * k], u[r + 3 * k], v);  // (U U^+)_{rc}
+        const double re = v.re - (r == c ? 1.0 : 0.0);
+        dev = fmax(dev, fmax(fabs(re), fabs(v.im)));
+      }
+    const Cx<double> det = u[0] * (u[4] * u[8] - u[7] * u[5]) - u[3] * (u[1] * u[8] - u[7] * u[2]) +
+                           u[6] * (u[1] * u[5] - u[4] * u[2]);
+    dev = fmax(dev, fmax(fabs(det.re - 1.0), fabs(det.im)));
+    m = fmaxf(m, (float)dev);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out_bits, __float_as_uint(m));
 }
 
 // max |re|, |im| over n complex entries (one atomicMax on the float bits;
@@ -269,16 +322,15 @@ __global__ void __launch_bounds__(256)
 }
 
 __global__ void __launch_bounds__(256)
-    clover_to_half_kernel(int4 *dst, int2 *tail, const double2 *src, int64_t V, float scale) {
+    clover_to_half_kernel(int4 *dst, int2 *tail, const double2 *src, int64_t V, int kexp) {
   const int64_t s = (int64_t)blockIdx.x * 256 + threadIdx.x;
   if (s >= V) return;
-  const float inv = scale > 0.f ? kInt16Scale / scale : 0.f;
+  const float inv = ldexpf(32768.0f, -kexp);
   for (int blk = 0; blk < 2; blk++) {
     int w[18];
     for (int k = 0; k < 18; k++) {
       const double2 t = src[(blk * 18 + k) * V + s];
-      const short lo = f2s((float)t.x * inv), hi = f2s((float)t.y * inv);
-      w[k] = ((int)(unsigned short)lo) | ((int)hi << 16);
+      w[k] = enc_pair((float)t.x * inv, (float)t.y * inv);
     }
     for (int k = 0; k < 4; k++) dst[(blk * 4 + k) * V + s] = make_int4(w[4 * k], w[4 * k + 1], w[4 * k + 2], w[4 * k + 3]);
     tail[blk * V + s] = make_int2(w[16], w[17]);

@@ -20,6 +20,7 @@
 // x += x_low, x_low = 0, r = b - D^+D x, r_low = r, rr = |r|^2.  Only the
 // FP64 true residual decides convergence.
 #pragma once
+#include "lmb_staggered.cuh"
 #include "lmb_wilson.cuh"
 
 namespace lmb {
@@ -115,9 +116,9 @@ LMB_D double sum_norm2(const Cx<R> *v, int n) {
 // ---------------------------------------------------------------------------
 // epilogues
 // ---------------------------------------------------------------------------
-template <int PS>
+template <int PS, int NC = 12>
 struct EpiStore {
-  Field<PS, 12> out;
+  Field<PS, NC> out;
   const int *status;  // optional: skip when != RUNNING
   LMB_D bool skip() const { return status && *(volatile const int *)status != ST_RUNNING; }
   template <typename R> LMB_D void operator()(int s, bool active, const Cx<R> *v) const {
@@ -125,9 +126,9 @@ struct EpiStore {
   }
 };
 
-template <int PS>
+template <int PS, int NC = 12>
 struct EpiStoreNorm {  // K1
-  Field<PS, 12> out;
+  Field<PS, NC> out;
   CGState *st;
   double *partials;
   unsigned *counter;
@@ -136,17 +137,17 @@ struct EpiStoreNorm {  // K1
     double n2[1] = {0.0}, tot[1];
     if (active) {
       out.store(s, v);
-      n2[0] = sum_norm2(v, 12);
+      n2[0] = sum_norm2(v, NC);
     }
     if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0)
       finalize_pAp(st, tot[0]);
   }
 };
 
-template <int PS, int PX>
+template <int PS, int PX, int NC = 12>
 struct EpiCGUpdate {  // K2
-  Field<PS, 12> p, r;
-  Field<PX, 12> x;
+  Field<PS, NC> p, r;
+  Field<PX, NC> x;
   CGState *st;
   double *partials;
   unsigned *counter;
@@ -155,18 +156,18 @@ struct EpiCGUpdate {  // K2
     double n2[1] = {0.0}, tot[1];
     if (active) {
       const R alpha = (R)st->alpha;
-      Cx<R> pv[12], rv[12], xv[12];
+      Cx<R> pv[NC], rv[NC], xv[NC];
       p.load(s, pv);
       r.load(s, rv);
       x.load(s, xv);
 #pragma unroll
-      for (int k = 0; k < 12; k++) {
+      for (int k = 0; k < NC; k++) {
         rv[k] = rv[k] - alpha * v[k];
         xv[k] = xv[k] + alpha * pv[k];
       }
       r.store(s, rv);
       x.store(s, xv);
-      n2[0] = sum_norm2(rv, 12);
+      n2[0] = sum_norm2(rv, NC);
     }
     if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0)
       finalize_rr(st, tot[0]);
@@ -174,10 +175,10 @@ struct EpiCGUpdate {  // K2
 };
 
 // r = b - v (FP64), r_low = r (optional), |r|^2 -> finalize_true(mode)
-template <int PS>
+template <int PS, int NC = 12>
 struct EpiTrueResidual {
-  Field<PREC_DOUBLE, 12> b, r;
-  Field<PS, 12> r_low;
+  Field<PREC_DOUBLE, NC> b, r;
+  Field<PS, NC> r_low;
   int write_low;
   int mode;
   CGState *st;
@@ -187,13 +188,13 @@ struct EpiTrueResidual {
   template <typename R> LMB_D void operator()(int s, bool active, const Cx<R> *v) const {
     double n2[1] = {0.0}, tot[1];
     if (active) {
-      Cx<double> bv[12], rv[12];
+      Cx<double> bv[NC], rv[NC];
       b.load(s, bv);
 #pragma unroll
-      for (int k = 0; k < 12; k++) rv[k] = Cx<double>(bv[k].re - (double)v[k].re, bv[k].im - (double)v[k].im);
+      for (int k = 0; k < NC; k++) rv[k] = Cx<double>(bv[k].re - (double)v[k].re, bv[k].im - (double)v[k].im);
       r.store(s, rv);
       if (write_low) r_low.store(s, rv);
-      n2[0] = sum_norm2(rv, 12);
+      n2[0] = sum_norm2(rv, NC);
     }
     if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0)
       finalize_true(st, tot[0], mode);

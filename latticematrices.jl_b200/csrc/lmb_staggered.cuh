@@ -1,0 +1,132 @@
+// lmb_staggered.cuh -- staggered and HISQ stencils on CUDA cores.
+//
+//   D psi = m psi + fc sum_mu eta_mu(x) [X_mu(x) psi(x+mu) - X_mu(x-mu)^+ psi(x-mu)]
+//                 + lc sum_mu eta_mu(x) [L_mu(x) psi(x+3mu) - L_mu(x-3mu)^+ psi(x-3mu)]
+// with fc = 1/2, lc = -(1+eps)/48 for D and both negated for D^+
+// (StaggeredDiracOperator.jl:1-17, 129-198; HISQDiracOperator.jl:55-72,
+// 269-357).  Plain staggered is the case without the Naik term.
+// eta_mu(x) = (-1)^(sum_{nu<mu} x_nu) with zero-based GLOBAL coordinates
+// (LinearAlgebras/staggered.jl:43-57): the rank offset is Geom::eta_off.
+// Fermion boundary phases: a wrap forward multiplies by phase, backward by
+// 1/phase, per wrap (a Naik hop on an extent below 3 may wrap twice).
+#pragma once
+#include "lmb_common.cuh"
+#include "lmb_wilson.cuh"
+
+namespace lmb {
+
+constexpr int kStagThreads = kDslashThreads;  // the epilogue reductions assume it
+
+// neighbour at signed distance d along mu with the number of edge crossings
+LMB_D int shift_site_any(const Geom &g, int s, const int *c, int mu, int d, int *wraps) {
+  const int L = g.L[mu];
+  int raw = c[mu] + d;
+  int w = 0;
+  while (raw >= L) {
+    raw -= L;
+    w++;
+  }
+  while (raw < 0) {
+    raw += L;
+    w--;
+  }
+  *wraps = w;
+  return s + (raw - c[mu]) * g.stride[mu];
+}
+
+template <typename R>
+LMB_D void apply_wraps(const Geom &g, int mu, int wraps, Cx<R> *v) {
+  if (!wraps || !((g.phase_mask >> mu) & 1)) return;
+  const double *ph = wraps > 0 ? g.ph_fwd[mu] : g.ph_bwd[mu];
+  const Cx<R> f((R)ph[0], (R)ph[1]);
+  const int n = wraps > 0 ? wraps : -wraps;
+  for (int k = 0; k < n; k++)
+#pragma unroll
+    for (int i = 0; i < 3; i++) v[i] = v[i] * f;
+}
+
+template <typename R>
+LMB_D void su3_mul_vec(const Cx<R> *u, const Cx<R> *v, Cx<R> *o) {
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    Cx<R> t = u[r] * v[0];
+    t = cfma(u[r + 3], v[1], t);
+    o[r] = cfma(u[r + 6], v[2], t);
+  }
+}
+template <typename R>
+LMB_D void su3_adj_mul_vec(const Cx<R> *u, const Cx<R> *v, Cx<R> *o) {
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    Cx<R> t = conj(u[3 * r]) * v[0];
+    t = cfma_conj(u[3 * r + 1], v[1], t);
+    o[r] = cfma_conj(u[3 * r + 2], v[2], t);
+  }
+}
+
+// forward minus backward hop of one direction at distance D, into acc
+template <typename R, int MU, int D, class SF, class G>
+LMB_D void stag_hop(const Geom &g, int s, const int *c, const SF &in, const G &U, R eta, Cx<R> *acc) {
+  Cx<R> v[3], u[9], o[3];
+  int w;
+  const int sp = (D == 1) ? fwd_site(g, s, c, MU, 1, &w) : shift_site_any(g, s, c, MU, D, &w);
+  in.load(sp, v);
+  apply_wraps(g, MU, w, v);
+  U.load(MU, s, u);
+  su3_mul_vec(u, v, o);
+#pragma unroll
+  for (int i = 0; i < 3; i++) acc[i] = acc[i] + eta * o[i];
+  int wb;
+  const int sm = (D == 1) ? bwd_site(g, s, c, MU, 1, &wb) : shift_site_any(g, s, c, MU, -D, &wb);
+  if (D == 1 && wb) wb = -1;
+  in.load(sm, v);
+  apply_wraps(g, MU, wb, v);
+  U.load(MU, sm, u);
+  su3_adj_mul_vec(u, v, o);
+#pragma unroll
+  for (int i = 0; i < 3; i++) acc[i] = acc[i] - eta * o[i];
+}
+
+struct NoLinks {
+  int64_t V;
+  template <typename R> LMB_D void load(int, int64_t, Cx<R> *) const {}
+};
+
+// Epi as for the Wilson kernel, on 3-component fields
+template <typename R, bool NAIK, class SF, class GF, class GL, class Epi>
+__global__ void __launch_bounds__(kStagThreads)
+    staggered_dslash_kernel(const Geom g, const SF in, const GF X, const GL Lk, const R mass, const R fc,
+                            const R lc, Epi epi) {
+  if (epi.skip()) return;
+  const int s = blockIdx.x * kStagThreads + threadIdx.x;
+  const bool active = s < g.V;
+  Cx<R> out[3];
+  if (active) {
+    int c[4];
+    site_coords(g, s, c);
+    const int p0 = c[0] + g.eta_off[0], p1 = p0 + c[1] + g.eta_off[1], p2 = p1 + c[2] + g.eta_off[2];
+    const R eta[4] = {(R)1, (p0 & 1) ? (R)-1 : (R)1, (p1 & 1) ? (R)-1 : (R)1, (p2 & 1) ? (R)-1 : (R)1};
+    Cx<R> fat[3] = {Cx<R>(0, 0), Cx<R>(0, 0), Cx<R>(0, 0)};
+    stag_hop<R, 0, 1>(g, s, c, in, X, eta[0], fat);
+    stag_hop<R, 1, 1>(g, s, c, in, X, eta[1], fat);
+    stag_hop<R, 2, 1>(g, s, c, in, X, eta[2], fat);
+    stag_hop<R, 3, 1>(g, s, c, in, X, eta[3], fat);
+    Cx<R> psi[3];
+    in.load(s, psi);
+    if constexpr (NAIK) {
+      Cx<R> lng[3] = {Cx<R>(0, 0), Cx<R>(0, 0), Cx<R>(0, 0)};
+      stag_hop<R, 0, 3>(g, s, c, in, Lk, eta[0], lng);
+      stag_hop<R, 1, 3>(g, s, c, in, Lk, eta[1], lng);
+      stag_hop<R, 2, 3>(g, s, c, in, Lk, eta[2], lng);
+      stag_hop<R, 3, 3>(g, s, c, in, Lk, eta[3], lng);
+#pragma unroll
+      for (int i = 0; i < 3; i++) out[i] = mass * psi[i] + fc * fat[i] + lc * lng[i];
+    } else {
+#pragma unroll
+      for (int i = 0; i < 3; i++) out[i] = mass * psi[i] + fc * fat[i];
+    }
+  }
+  epi(s, active, out);
+}
+
+}  // namespace lmb

@@ -20,7 +20,15 @@
 
 namespace lmb {
 
-constexpr int kDslashThreads = 128;
+// threads per block and the minimum resident blocks per SM requested from
+// the register allocator (0 = no request); set at compile time
+#ifndef LMB_DSLASH_THREADS
+#define LMB_DSLASH_THREADS 128
+#endif
+#ifndef LMB_DSLASH_MINB
+#define LMB_DSLASH_MINB 0
+#endif
+constexpr int kDslashThreads = LMB_DSLASH_THREADS;
 
 // half-spin projection rows of (1 + PM g_mu) psi (WilsonDiracOperator.jl:157-175)
 template <int PM, int MU, typename R>
@@ -160,7 +168,7 @@ struct NoClover {
 //   bool skip() const                      -- whole grid exits (paused solve)
 //   void operator()(s, active, out[12])    -- consume the result
 template <typename R, int DAG, bool CLOVER, class SF, class G, class CL, class Epi>
-__global__ void __launch_bounds__(kDslashThreads)
+__global__ void __launch_bounds__(kDslashThreads, LMB_DSLASH_MINB)
     wilson_dslash_kernel(const Geom g, const SF in, const G U, const CL A,
                          const R kappa, Epi epi) {
   if (epi.skip()) return;

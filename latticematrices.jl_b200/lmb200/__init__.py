@@ -10,8 +10,14 @@ from .lattice import (LatticeMatrix, clear_matrix_, halo_is_dirty,  # noqa: F401
                       mark_halo_dirty_, similar, substitute_)
 from .operators import (CloverFieldStrength4D, WilsonDiracCloverOperator4D,  # noqa: F401
                         WilsonDiracOperator4D, adjoint, mul_,
+                        StaggeredDiracOperator4D, HISQLinks4D,
+                        HISQDiracOperator4D,
                         mul_cached_clover_, mul_cached_clover_adjoint_,
                         update_clover_)
+from .hisq import (HISQDiracCache4D, hisq_fat7_level1_,  # noqa: F401
+                   hisq_fat7_level2_, hisq_links_from_thin, hisq_naik_links_,
+                   hisq_project_u3_, mul_cached_hisq_,
+                   mul_cached_hisq_adjoint_)
 from .inputs import gaussian_fermion, random_su3_links  # noqa: F401
 from .solver import (CGResult, DdagDOp, cg_, dot, pseudofermion_action,  # noqa: F401
                      solve_)

@@ -11,7 +11,8 @@ import os
 import threading
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "liblmb200.so")
+# LMB200_LIB selects another build of the library (e.g. a tuning variant)
+LIB_PATH = os.environ.get("LMB200_LIB", os.path.join(_HERE, "liblmb200.so"))
 
 LMB_OK = 0
 LMB_ERR_ARG = -1
@@ -32,7 +33,9 @@ EXPORTED = (
     "lmb_set_geometry", "lmb_links_upload", "lmb_wilson_apply",
     "lmb_wilson_clover_apply", "lmb_clover_field_strength", "lmb_cg_ddagd",
     "lmb_field_dot", "lmb_random_su3_links", "lmb_gaussian_field",
-    "lmb_field_dot_noalloc",
+    "lmb_field_dot_noalloc", "lmb_staggered_apply", "lmb_hisq_apply",
+    "lmb_hisq_fat7", "lmb_hisq_project_u3", "lmb_hisq_naik",
+    "lmb_hisq_links_from_thin",
 )
 
 
@@ -64,7 +67,7 @@ class CGResultC(ctypes.Structure):
         ("true_residual_norm", ctypes.c_double),
         ("dslash_ms", ctypes.c_double), ("update_ms", ctypes.c_double),
         ("dslash_launches", ctypes.c_int), ("update_launches", ctypes.c_int),
-        ("kernel_launches", ctypes.c_longlong),
+        ("kernel_launches", ctypes.c_longlong), ("link_reals", ctypes.c_int),
     ]
 
 
@@ -103,6 +106,18 @@ def load(path: str = LIB_PATH):
             vp, vp, vp, ctypes.c_double, ctypes.c_double, ctypes.c_int,
             ctypes.c_int, vp]
         lib.lmb_clover_field_strength.argtypes = [vp, ctypes.POINTER(vp), vp]
+        lib.lmb_staggered_apply.argtypes = [vp, vp, vp, ctypes.c_double,
+                                            ctypes.c_int, ctypes.c_int, vp]
+        lib.lmb_hisq_apply.argtypes = [vp, vp, vp, ctypes.c_double,
+                                       ctypes.c_double, ctypes.c_int,
+                                       ctypes.c_int, vp]
+        pvp = ctypes.POINTER(vp)
+        lib.lmb_hisq_fat7.argtypes = [vp, pvp, dp, pvp, vp]
+        lib.lmb_hisq_project_u3.argtypes = [vp, pvp, pvp, vp]
+        lib.lmb_hisq_naik.argtypes = [vp, pvp, pvp, vp]
+        lib.lmb_hisq_links_from_thin.argtypes = [
+            vp, pvp, ctypes.POINTER(ctypes.c_uint64), ctypes.c_double, pvp,
+            pvp, vp]
         lib.lmb_cg_ddagd.argtypes = [vp, ctypes.POINTER(CGParams), vp, vp,
                                      ctypes.POINTER(CGResultC), vp]
         lib.lmb_field_dot.argtypes = [vp, vp, vp, ctypes.c_int, dp, vp]

@@ -11,6 +11,8 @@ from __future__ import annotations
 
 import ctypes
 
+import numpy as np
+
 from ._lib import (ArgumentError, Context, LINKS_THIN, PREC)
 from .lattice import LatticeMatrix, mark_halo_dirty_
 
@@ -242,3 +244,166 @@ def mul_cached_clover_adjoint_(result, cache, U1, U2, U3, U4, psi):
     """mul_cached_clover_adjoint! (WilsonDiracCloverOperator.jl:653-668)."""
     update_clover_(cache, [U1, U2, U3, U4])
     return mul_(result, adjoint(cache), psi)
+
+
+# ---------------------------------------------------------------------------
+# staggered and HISQ
+# ---------------------------------------------------------------------------
+def _validate_staggered_links(U, label="gauge link U"):
+    """_validate_staggered_gauge_links (StaggeredDiracOperator.jl:23-45)."""
+    if len(U) != 4:
+        raise ArgumentError("U must be a vector of length 4")
+    ref = U[0]
+    if ref.NC1 != ref.NC2:
+        raise ArgumentError("staggered gauge links must be square matrices")
+    for mu, link in enumerate(U, start=1):
+        if (link.NC1, link.NC2) != (ref.NC1, ref.NC2):
+            raise ArgumentError("all gauge links must have the same matrix size")
+        if link.gsize != ref.gsize:
+            raise ArgumentError("all gauge links must have the same global lattice size")
+        if link.nw != ref.nw:
+            raise ArgumentError("all gauge links must have the same halo width")
+        if any(p != 1 for p in link.phases):
+            raise ArgumentError(f"{label}[{mu}] must use periodic boundary phases")
+
+
+def _validate_staggered_application(result, links, psi, what="gauge link U"):
+    """_validate_staggered_application (StaggeredDiracOperator.jl:66-92)."""
+    if result is psi:
+        raise ArgumentError("staggered mul! requires distinct result and input fields")
+    if not result.same_geometry(psi):
+        raise ArgumentError("result and fermion fields must use the same lattice geometry")
+    if result.phases != psi.phases:
+        raise ArgumentError("result and fermion fields must use the same boundary phases")
+    tol = np.sqrt(np.finfo(np.float32 if psi.elementtype == np.complex64
+                           else np.float64).eps)
+    for mu, ph in enumerate(psi.phases, start=1):
+        if not np.isclose(abs(complex(ph)), 1.0, atol=tol, rtol=tol):
+            raise ArgumentError(f"fermion boundary phase {mu} must have unit magnitude")
+    if psi.NC2 != 1 or result.NC2 != 1:
+        raise ArgumentError("staggered fields have one spin component per site")
+    for mu, link in enumerate(links, start=1):
+        if link.NC1 != psi.NC1:
+            raise ArgumentError(
+                f"{what}[{mu}] and fermion field have different color sizes")
+        if link.elementtype != psi.elementtype:
+            raise ArgumentError(
+                f"{what}[{mu}] and fermion field have different element types")
+        if link.gsize != psi.gsize or link.nw != psi.nw:
+            raise ArgumentError(
+                f"{what}[{mu}] and fermion field use different lattice geometry")
+    if psi.NC1 != _NC_SUPPORTED:
+        raise ArgumentError(
+            f"the sm_100a kernels implement NC={_NC_SUPPORTED}; got NC={psi.NC1}")
+
+
+class StaggeredDiracOperator4D(_LinkOperator):
+    """One-link staggered operator, Bridge++ normalisation
+    (StaggeredDiracOperator.jl:1-55)."""
+
+    def __init__(self, U, mass):
+        _validate_staggered_links(U)
+        super().__init__(U)
+        mass = float(mass)
+        if not np.isfinite(mass):
+            raise ArgumentError("mass must be finite")
+        self.mass = mass
+
+    def adjoint(self):
+        return _AdjointApply(self)
+
+    def _apply(self, out, psi, dagger, precision):
+        _validate_staggered_application(out, self.U, psi)
+        st = _stream()
+        ctx = self._bind(psi, st)
+        ctx.check(ctx.lib.lmb_staggered_apply(
+            ctx.handle, out.data_ptr(), psi.data_ptr(), self.mass,
+            int(dagger), PREC[precision], st))
+        mark_halo_dirty_(out)
+        return out
+
+
+class _AdjointApply(_Adjoint):
+    def _apply(self, out, psi, dagger, precision):
+        return self.parent._apply(out, psi, not dagger, precision)
+
+
+class HISQLinks4D:
+    """Fat links X_mu and forward-anchored Naik links L_mu
+    (HISQDiracOperator.jl:1-53)."""
+
+    def __init__(self, fat_links, long_links):
+        _validate_staggered_links(fat_links, "fat link X")
+        _validate_staggered_links(long_links, "long link L")
+        ref = fat_links[0]
+        for mu, link in enumerate(long_links, start=1):
+            if (link.NC1, link.NC2) != (ref.NC1, ref.NC2):
+                raise ArgumentError(
+                    f"long link L[{mu}] and fat links have different matrix sizes")
+            if link.gsize != ref.gsize or link.nw != ref.nw:
+                raise ArgumentError(
+                    f"long link L[{mu}] and fat links use different lattice geometry")
+            if link.elementtype != ref.elementtype:
+                raise ArgumentError(
+                    f"long link L[{mu}] and fat links have different element types")
+        nw = ref.nw
+        if not (nw == 0 or nw >= 3):
+            raise ArgumentError(
+                "HISQ links require nw=0 or nw>=3 for the three-hop Naik term")
+        if nw and any(extent < nw for extent in ref.gsize):
+            raise ArgumentError(
+                f"each local lattice extent must be at least the halo width nw={nw}")
+        self.fat_links = list(fat_links)
+        self.long_links = list(long_links)
+
+
+class HISQDiracOperator4D:
+    """HISQ stencil (HISQDiracOperator.jl:55-110):
+    m psi + sum eta {1/2 [X psi(x+mu) - X' psi(x-mu)]
+                     - (1+eps)/48 [L psi(x+3mu) - L' psi(x-3mu)]}."""
+
+    def __init__(self, links, mass, naik_epsilon=0.0):
+        if not isinstance(links, HISQLinks4D):
+            raise ArgumentError("HISQDiracOperator4D needs HISQLinks4D")
+        mass, eps = float(mass), float(naik_epsilon)
+        if not np.isfinite(mass):
+            raise ArgumentError("mass must be finite")
+        if not np.isfinite(eps):
+            raise ArgumentError("naik_epsilon must be finite")
+        self.links = links
+        self.mass = mass
+        self.naik_epsilon = eps
+        self._ctx = None
+
+    @property
+    def ctx(self):
+        if self._ctx is None:
+            dev = self.links.fat_links[0].A.device
+            self._ctx = Context(dev.index or 0)
+        return self._ctx
+
+    def adjoint(self):
+        return _AdjointApply(self)
+
+    def _bind(self, psi, stream):
+        from ._lib import LINKS_FAT, LINKS_LONG
+        ctx = self.ctx
+        ctx.set_geometry(psi.gsize, psi.nw, psi.phases, psi.coords,
+                         psi.dtype_code)
+        for which, links in ((LINKS_FAT, self.links.fat_links),
+                             (LINKS_LONG, self.links.long_links)):
+            ctx.upload_links(which, [u.data_ptr() for u in links],
+                             [u.halo_epoch.core for u in links], stream)
+        return ctx
+
+    def _apply(self, out, psi, dagger, precision):
+        _validate_staggered_application(
+            out, self.links.fat_links + self.links.long_links, psi,
+            "fat link X")
+        st = _stream()
+        ctx = self._bind(psi, st)
+        ctx.check(ctx.lib.lmb_hisq_apply(
+            ctx.handle, out.data_ptr(), psi.data_ptr(), self.mass,
+            self.naik_epsilon, int(dagger), PREC[precision], st))
+        mark_halo_dirty_(out)
+        return out

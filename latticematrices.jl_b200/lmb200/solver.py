@@ -15,9 +15,10 @@ import math
 from dataclasses import dataclass
 
 from ._lib import (ArgumentError, CG_REASONS, CGParams, CGResultC, PREC,
-                   OP_WILSON, OP_WILSON_CLOVER)
+                   OP_HISQ, OP_STAGGERED, OP_WILSON, OP_WILSON_CLOVER)
 from .lattice import LatticeMatrix, mark_halo_dirty_
-from .operators import (WilsonDiracCloverOperator4D, WilsonDiracOperator4D,
+from .operators import (HISQDiracOperator4D, StaggeredDiracOperator4D,
+                        WilsonDiracCloverOperator4D, WilsonDiracOperator4D,
                         _stream, adjoint, mul_)
 
 
@@ -36,6 +37,7 @@ class CGResult:
     dslash_launches: int = 0
     update_launches: int = 0
     kernel_launches: int = 0
+    link_reals: int = 18
 
 
 class DdagDOp:
@@ -88,6 +90,13 @@ def _native_operator(A):
         return D, OP_WILSON_CLOVER
     if isinstance(D, WilsonDiracOperator4D):
         return D, OP_WILSON
+    if isinstance(D, StaggeredDiracOperator4D):
+        return D, OP_STAGGERED
+    if isinstance(D, HISQDiracOperator4D):
+        return D, OP_HISQ
+    from .hisq import HISQDiracCache4D
+    if isinstance(D, HISQDiracCache4D):
+        return D, OP_HISQ
     return None
 
 
@@ -101,18 +110,20 @@ def cg_(x, A, b, r=None, p=None, Ap=None, *, rtol=1e-10, atol=0.0,
     native = _native_operator(A)
     if native is not None:
         D, op = native
-        wilson = D.wilson if op == OP_WILSON_CLOVER else D
+        binder = D.wilson if op == OP_WILSON_CLOVER else D
         prm = CGParams()
         prm.op = op
-        prm.kappa = D.kappa
+        prm.kappa = getattr(D, "kappa", 0.0)
         prm.csw = getattr(D, "cSW", 0.0)
+        prm.mass = getattr(D, "mass", 0.0)
+        prm.naik_epsilon = getattr(D, "naik_epsilon", 0.0)
         prm.rtol, prm.atol, prm.maxiter = float(rtol), float(atol), int(maxiter)
         prm.precision = PREC[precision]
         prm.delta = float(delta)
         prm.check_interval = int(check_interval)
         prm.profile = int(bool(profile))
         st = _stream()
-        ctx = wilson._bind(b, st)
+        ctx = binder._bind(b, st)
         res = CGResultC()
         ctx.check(ctx.lib.lmb_cg_ddagd(ctx.handle, ctypes.byref(prm),
                                        x.data_ptr(), b.data_ptr(),
@@ -122,7 +133,8 @@ def cg_(x, A, b, r=None, p=None, Ap=None, *, rtol=1e-10, atol=0.0,
                         res.relative_residual, CG_REASONS[res.reason],
                         res.reliable_updates, res.true_residual_norm,
                         res.dslash_ms, res.update_ms, res.dslash_launches,
-                        res.update_launches, res.kernel_launches)
+                        res.update_launches, res.kernel_launches,
+                        res.link_reals)
     if precision != "double":
         raise ArgumentError("mixed precision needs a native DdagDOp operator")
     return _cg_generic(x, A, b, r, p, Ap, rtol, atol, maxiter)
