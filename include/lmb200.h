@@ -184,6 +184,41 @@ int lmb_clover_field_strength(lmb_ctx *ctx, void *const F[6], void *stream);
 int lmb_cg_ddagd(lmb_ctx *ctx, const lmb_cg_params *params, void *x,
                  const void *b, lmb_cg_result *result, void *stream);
 
+/* Batched D'D CG: several lattices of different sizes, each with several
+ * right-hand sides, solved together (no reference counterpart: the reference
+ * solves one right-hand side per cg! call, cg.jl:73-137, which this applies
+ * to every right-hand side).  Wilson operator, FP32 inner iterations with
+ * FP64 reliable updates (params->precision = LMB_PREC_SINGLE) and an FP64
+ * true-residual stop per right-hand side.  One launch per CG stage covers
+ * all lattices and right-hand sides; an iteration is replayed from a CUDA
+ * graph; the right-hand-side block and threads per block are autotuned on
+ * the first call for a given set of lattice shapes and cached in the
+ * context.  Links must be SU(3).  results has one entry per right-hand side
+ * (lattice-major). */
+typedef struct {
+  int L[4];
+  int nw;
+  double phase_re[4], phase_im[4];
+  const void *U[4];   /* ComplexF64 padded gauge links */
+  uint64_t epoch[4];  /* halo_epoch.core of the links (cache key) */
+  double kappa;
+  int nrhs;
+  void *const *x;     /* nrhs ComplexF64 padded fields: guess in, solution out */
+  const void *const *b;
+} lmb_batch_lattice;
+
+typedef struct {
+  int rhs_block;            /* right-hand sides sharing each link load */
+  int threads;              /* sites per block */
+  double ms_per_iteration;  /* device time of one batched CG iteration */
+  int graph_iterations;     /* iterations replayed from the CUDA graph */
+} lmb_batch_tuning;
+
+int lmb_cg_ddagd_batched(lmb_ctx *ctx, const lmb_cg_params *params,
+                         int nlattices, const lmb_batch_lattice *lattices,
+                         lmb_cg_result *results, lmb_batch_tuning *tuning,
+                         void *stream);
+
 /* dot(a, b) = sum conj(a) b over the core (LinearAlgebras/linearalgebra_D.jl:
  * 3325-3341) of two padded fields with ncomp complex numbers per site.
  * out[0] = Re, out[1] = Im.  Synchronises the stream. */

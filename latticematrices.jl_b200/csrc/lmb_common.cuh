@@ -438,7 +438,18 @@ template <> struct Clover<PREC_HALF> {
 // all partials in block order and returns true (others false).
 // ---------------------------------------------------------------------------
 template <int NT, int N>
+LMB_D bool grid_reduce_slots(double (&v)[N], double *partials, unsigned *counter, double (&total)[N],
+                             unsigned slot, unsigned nslots);
+
+template <int NT, int N>
 LMB_D bool grid_reduce(double (&v)[N], double *partials, unsigned *counter, double (&total)[N]) {
+  return grid_reduce_slots<NT, N>(v, partials, counter, total, blockIdx.x, gridDim.x);
+}
+
+// as grid_reduce, for `nslots` cooperating blocks of which this is `slot`
+template <int NT, int N>
+LMB_D bool grid_reduce_slots(double (&v)[N], double *partials, unsigned *counter, double (&total)[N],
+                             unsigned slot, unsigned nslots) {
   __shared__ double red[N][NT / 32];
   __shared__ bool last;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -455,11 +466,11 @@ LMB_D bool grid_reduce(double (&v)[N], double *partials, unsigned *counter, doub
     for (int n = 0; n < N; n++) {
       double x = 0;
       for (int w = 0; w < NT / 32; w++) x += red[n][w];
-      partials[(size_t)N * blockIdx.x + n] = x;
+      partials[(size_t)N * slot + n] = x;
     }
     __threadfence();
     unsigned ticket = atomicAdd(counter, 1u);
-    last = (ticket == gridDim.x - 1);
+    last = (ticket == nslots - 1);
   }
   __syncthreads();
   if (!last) return false;
@@ -467,7 +478,7 @@ LMB_D bool grid_reduce(double (&v)[N], double *partials, unsigned *counter, doub
 #pragma unroll
   for (int n = 0; n < N; n++) {
     double x = 0;
-    for (unsigned b = threadIdx.x; b < gridDim.x; b += NT)
+    for (unsigned b = threadIdx.x; b < nslots; b += NT)
       x += ((volatile double *)partials)[(size_t)N * b + n];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);

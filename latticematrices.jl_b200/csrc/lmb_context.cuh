@@ -5,8 +5,10 @@
 
 #include <cstdarg>
 #include <cstdio>
+#include <deque>
 #include <map>
 #include <string>
+#include <vector>
 
 #include "../../include/lmb200.h"
 #include "lmb_pack.cuh"
@@ -58,8 +60,23 @@ struct lmb_smear_key {
   bool valid = false;
 };
 
+struct lmb_batch_links {
+  const void *ptr[4] = {nullptr, nullptr, nullptr, nullptr};
+  uint64_t epoch[4] = {0, 0, 0, 0};
+  int64_t V = 0;
+  double2 *d12 = nullptr;  // FP64 reconstruct-12
+  float4 *f12 = nullptr;   // FP32 reconstruct-12
+};
+
+struct lmb_batch_tune {
+  int nb = 0, nt = 0;
+  double ms = 0;
+};
+
 struct lmb_ctx {
   int device = 0;
+  std::deque<lmb_batch_links> batch_links;  // deque: element addresses stay valid on growth
+  std::map<std::string, lmb_batch_tune> batch_tune;
   lmb_smear_key smear;  // thin links the HISQ fat/long link sets were built from
   bool geom_set = false;
   lmb::Geom g{};

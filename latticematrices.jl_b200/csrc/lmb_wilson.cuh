@@ -164,6 +164,24 @@ struct NoClover {
   int64_t V;
 };
 
+// D psi at site s (plain Wilson: A = 1)
+template <typename R, int DAG, class SF, class G>
+LMB_D void wilson_site(const Geom &g, int s, const SF &in, const G &U, R kappa, Cx<R> *out) {
+  int c[4];
+  site_coords(g, s, c);
+  Cx<R> acc[12];
+#pragma unroll
+  for (int k = 0; k < 12; k++) acc[k] = Cx<R>(0, 0);
+  hop_dir<R, DAG, 0>(g, s, c, in, U, acc);
+  hop_dir<R, DAG, 1>(g, s, c, in, U, acc);
+  hop_dir<R, DAG, 2>(g, s, c, in, U, acc);
+  hop_dir<R, DAG, 3>(g, s, c, in, U, acc);
+  Cx<R> p[12];
+  in.load(s, p);
+#pragma unroll
+  for (int k = 0; k < 12; k++) out[k] = p[k] - kappa * acc[k];
+}
+
 // The Wilson(-clover) kernel.  Epi must provide:
 //   bool skip() const                      -- whole grid exits (paused solve)
 //   void operator()(s, active, out[12])    -- consume the result

@@ -19,5 +19,5 @@ from .hisq import (HISQDiracCache4D, hisq_fat7_level1_,  # noqa: F401
                    hisq_project_u3_, mul_cached_hisq_,
                    mul_cached_hisq_adjoint_)
 from .inputs import gaussian_fermion, random_su3_links  # noqa: F401
-from .solver import (CGResult, DdagDOp, cg_, dot, pseudofermion_action,  # noqa: F401
-                     solve_)
+from .solver import (CGResult, DdagDOp, cg_, cg_batched_, dot,  # noqa: F401
+                     pseudofermion_action, solve_)

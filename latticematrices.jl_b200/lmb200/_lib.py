@@ -35,7 +35,7 @@ EXPORTED = (
     "lmb_field_dot", "lmb_random_su3_links", "lmb_gaussian_field",
     "lmb_field_dot_noalloc", "lmb_staggered_apply", "lmb_hisq_apply",
     "lmb_hisq_fat7", "lmb_hisq_project_u3", "lmb_hisq_naik",
-    "lmb_hisq_links_from_thin",
+    "lmb_hisq_links_from_thin", "lmb_cg_ddagd_batched",
 )
 
 
@@ -68,6 +68,25 @@ class CGResultC(ctypes.Structure):
         ("dslash_ms", ctypes.c_double), ("update_ms", ctypes.c_double),
         ("dslash_launches", ctypes.c_int), ("update_launches", ctypes.c_int),
         ("kernel_launches", ctypes.c_longlong), ("link_reals", ctypes.c_int),
+    ]
+
+
+class BatchLattice(ctypes.Structure):
+    _fields_ = [
+        ("L", ctypes.c_int * 4), ("nw", ctypes.c_int),
+        ("phase_re", ctypes.c_double * 4), ("phase_im", ctypes.c_double * 4),
+        ("U", ctypes.c_void_p * 4), ("epoch", ctypes.c_uint64 * 4),
+        ("kappa", ctypes.c_double), ("nrhs", ctypes.c_int),
+        ("x", ctypes.POINTER(ctypes.c_void_p)),
+        ("b", ctypes.POINTER(ctypes.c_void_p)),
+    ]
+
+
+class BatchTuning(ctypes.Structure):
+    _fields_ = [
+        ("rhs_block", ctypes.c_int), ("threads", ctypes.c_int),
+        ("ms_per_iteration", ctypes.c_double),
+        ("graph_iterations", ctypes.c_int),
     ]
 
 
@@ -115,6 +134,10 @@ def load(path: str = LIB_PATH):
         lib.lmb_hisq_fat7.argtypes = [vp, pvp, dp, pvp, vp]
         lib.lmb_hisq_project_u3.argtypes = [vp, pvp, pvp, vp]
         lib.lmb_hisq_naik.argtypes = [vp, pvp, pvp, vp]
+        lib.lmb_cg_ddagd_batched.argtypes = [
+            vp, ctypes.POINTER(CGParams), ctypes.c_int,
+            ctypes.POINTER(BatchLattice), ctypes.POINTER(CGResultC),
+            ctypes.POINTER(BatchTuning), vp]
         lib.lmb_hisq_links_from_thin.argtypes = [
             vp, pvp, ctypes.POINTER(ctypes.c_uint64), ctypes.c_double, pvp,
             pvp, vp]

@@ -14,6 +14,8 @@ import ctypes
 import math
 from dataclasses import dataclass
 
+import numpy as np
+
 from ._lib import (ArgumentError, CG_REASONS, CGParams, CGResultC, PREC,
                    OP_HISQ, OP_STAGGERED, OP_WILSON, OP_WILSON_CLOVER)
 from .lattice import LatticeMatrix, mark_halo_dirty_
@@ -236,3 +238,72 @@ def pseudofermion_action(D, phi, eta, Deta, r, p, Ap, **kwargs):
             f"CG failed with reason {res.reason} after {res.iterations} "
             f"iterations; relative residual = {res.relative_residual}")
     return dot(phi, eta).real
+
+
+def cg_batched_(systems, *, rtol=1e-10, atol=0.0, maxiter=5000, delta=0.1,
+                check_interval=0, precision="single"):
+    """Solve D'D x = b for every (x, b) of every system in one batched CG
+    (lmb_cg_ddagd_batched): systems = [(WilsonDiracOperator4D, [(x, b), ...]),
+    ...], lattices of any sizes.  FP32 inner iterations with FP64 reliable
+    updates; each right-hand side stops on its own FP64 true residual.
+    Returns (list of CGResult per right-hand side, tuning dict)."""
+    from ._lib import BatchLattice, BatchTuning
+    if precision != "single":
+        raise ArgumentError("the batched CG runs FP32 inner iterations")
+    if not systems:
+        raise ArgumentError("no systems")
+    lats = (BatchLattice * len(systems))()
+    keep = []
+    ctx = None
+    st = _stream()
+    total = 0
+    for i, (D, pairs) in enumerate(systems):
+        if not isinstance(D, WilsonDiracOperator4D):
+            raise ArgumentError("the batched CG is built for WilsonDiracOperator4D")
+        if not pairs:
+            raise ArgumentError("a system needs at least one right-hand side")
+        for x, b in pairs:
+            _validate_cg_arguments(x, b, None, None, None, rtol, atol, maxiter)
+            if not x.same_geometry(b) or x.phases != b.phases:
+                raise ArgumentError("x and b must share geometry and phases")
+            if x.elementtype != np.complex128:
+                raise ArgumentError("the batched CG takes ComplexF64 fields")
+        b0 = pairs[0][1]
+        lat = lats[i]
+        lat.L = (ctypes.c_int * 4)(*b0.gsize)
+        lat.nw = b0.nw
+        lat.phase_re = (ctypes.c_double * 4)(*[complex(p).real for p in b0.phases])
+        lat.phase_im = (ctypes.c_double * 4)(*[complex(p).imag for p in b0.phases])
+        lat.U = (ctypes.c_void_p * 4)(*[u.data_ptr() for u in D.U])
+        lat.epoch = (ctypes.c_uint64 * 4)(*[u.halo_epoch.core for u in D.U])
+        lat.kappa = D.kappa
+        lat.nrhs = len(pairs)
+        xs = (ctypes.c_void_p * len(pairs))(*[x.data_ptr() for x, _ in pairs])
+        bs = (ctypes.c_void_p * len(pairs))(*[b.data_ptr() for _, b in pairs])
+        keep += [xs, bs]
+        lat.x = ctypes.cast(xs, ctypes.POINTER(ctypes.c_void_p))
+        lat.b = ctypes.cast(bs, ctypes.POINTER(ctypes.c_void_p))
+        total += len(pairs)
+        ctx = ctx or D.ctx
+    prm = CGParams()
+    prm.op = 0
+    prm.kappa = 0.0
+    prm.rtol, prm.atol, prm.maxiter = float(rtol), float(atol), int(maxiter)
+    prm.precision = PREC["single"]
+    prm.delta = float(delta)
+    prm.check_interval = int(check_interval)
+    res = (CGResultC * total)()
+    tun = BatchTuning()
+    ctx.check(ctx.lib.lmb_cg_ddagd_batched(ctx.handle, ctypes.byref(prm),
+                                           len(systems), lats, res,
+                                           ctypes.byref(tun), st))
+    for _, pairs in systems:
+        for x, _ in pairs:
+            mark_halo_dirty_(x)
+    out = [CGResult(bool(r.converged), r.iterations, r.residual_norm,
+                    r.relative_residual, CG_REASONS[r.reason],
+                    r.reliable_updates, r.true_residual_norm,
+                    link_reals=r.link_reals) for r in res]
+    return out, dict(rhs_block=tun.rhs_block, threads=tun.threads,
+                     ms_per_iteration=tun.ms_per_iteration,
+                     graph_iterations=tun.graph_iterations)
