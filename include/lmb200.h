@@ -171,6 +171,28 @@ int lmb_hisq_links_from_thin(lmb_ctx *ctx, const void *const U[4],
                              void *const X[4], void *const L[4],
                              void *stream);
 
+/* hisq_link_pullback!(dU, cache, U, result_cotangent, psi; coefficient)
+ * (Operators/HISQPullback.jl:620-699): accumulates into the four padded thin-
+ * link fields dU the gradient G of f = coefficient Re<result_cotangent,
+ * D_HISQ(U) psi> through Naik, level-2 Fat7 + Lepage, U(3) projection and
+ * level-1 Fat7 (df = Re sum conj(G) dU).  The smearing levels and staples are
+ * recomputed from U, not stored.  FP64. */
+int lmb_hisq_link_pullback(lmb_ctx *ctx, const void *const U[4],
+                           double naik_epsilon, double coefficient,
+                           const void *result_cotangent, const void *psi,
+                           void *const dU[4], void *stream);
+
+/* Fermion force dS/dU of S = phi^+ (D^+D)^-1 phi for the HISQ operator built
+ * from thin links U (dSFdU, ext/LatticeMatricesEnzymeExt.jl:387-460): solves
+ * eta = (D^+D)^-1 phi with lmb_cg_ddagd (cg->precision, rtol, ...), chi =
+ * D eta, then accumulates -2 d/dU Re<chi, D(U) eta> into dU.  result receives
+ * the CG status. */
+int lmb_hisq_fermion_force(lmb_ctx *ctx, const void *const U[4],
+                           const uint64_t epoch[4], double mass,
+                           double naik_epsilon, const void *phi,
+                           void *const dU[4], const lmb_cg_params *cg,
+                           lmb_cg_result *result, void *stream);
+
 /* CloverFieldStrength4D(U) components (12,13,14,23,24,34) written to six
  * padded (3,3,...) fields (Operators/WilsonDiracCloverOperator.jl:28-35,
  * 392-399). */

@@ -15,6 +15,7 @@ from .operators import (CloverFieldStrength4D, WilsonDiracCloverOperator4D,  # n
                         mul_cached_clover_, mul_cached_clover_adjoint_,
                         update_clover_)
 from .hisq import (HISQDiracCache4D, hisq_fat7_level1_,  # noqa: F401
+                   hisq_fermion_force_, hisq_link_pullback_,
                    hisq_fat7_level2_, hisq_links_from_thin, hisq_naik_links_,
                    hisq_project_u3_, mul_cached_hisq_,
                    mul_cached_hisq_adjoint_)

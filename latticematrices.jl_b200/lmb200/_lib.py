@@ -36,6 +36,7 @@ EXPORTED = (
     "lmb_field_dot_noalloc", "lmb_staggered_apply", "lmb_hisq_apply",
     "lmb_hisq_fat7", "lmb_hisq_project_u3", "lmb_hisq_naik",
     "lmb_hisq_links_from_thin", "lmb_cg_ddagd_batched",
+    "lmb_hisq_link_pullback", "lmb_hisq_fermion_force",
 )
 
 
@@ -138,6 +139,13 @@ def load(path: str = LIB_PATH):
             vp, ctypes.POINTER(CGParams), ctypes.c_int,
             ctypes.POINTER(BatchLattice), ctypes.POINTER(CGResultC),
             ctypes.POINTER(BatchTuning), vp]
+        lib.lmb_hisq_link_pullback.argtypes = [
+            vp, ctypes.POINTER(vp), ctypes.c_double, ctypes.c_double, vp, vp,
+            ctypes.POINTER(vp), vp]
+        lib.lmb_hisq_fermion_force.argtypes = [
+            vp, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_uint64),
+            ctypes.c_double, ctypes.c_double, vp, ctypes.POINTER(vp),
+            ctypes.POINTER(CGParams), ctypes.POINTER(CGResultC), vp]
         lib.lmb_hisq_links_from_thin.argtypes = [
             vp, pvp, ctypes.POINTER(ctypes.c_uint64), ctypes.c_double, pvp,
             pvp, vp]

@@ -191,3 +191,78 @@ def mul_cached_hisq_adjoint_(result, cache, U1, U2, U3, U4, psi):
     from .operators import adjoint, mul_
     cache.update_([U1, U2, U3, U4])
     return mul_(result, adjoint(cache), psi)
+
+
+def _validate_pullback(dthin_links, thin_links, result_cotangent, psi):
+    """_validate_hisq_link_pullback (HISQPullback.jl:560-618)."""
+    if len(dthin_links) != 4:
+        raise ArgumentError("HISQ link pullback requires four thin-link cotangents")
+    ref = thin_links[0]
+    if (ref.NC1, ref.NC2) != (3, 3):
+        raise ArgumentError("HISQ link pullback currently requires three-color thin links")
+    if ref.nw < 3 and ref.nw != 0:
+        raise ArgumentError("HISQ link pullback requires halo width nw >= 3")
+    if (result_cotangent.NC1, result_cotangent.NC2, psi.NC1, psi.NC2) != (3, 1, 3, 1):
+        raise ArgumentError(
+            "HISQ link pullback requires three-color one-column fermion fields")
+    if not result_cotangent.same_geometry(psi) or result_cotangent.phases != psi.phases:
+        raise ArgumentError(
+            "HISQ result cotangent and source must share geometry and boundary phases")
+    if ref.gsize != psi.gsize or ref.nw != psi.nw:
+        raise ArgumentError(
+            "HISQ thin links and fermion fields must share one lattice geometry")
+    if not (ref.elementtype == psi.elementtype == result_cotangent.elementtype):
+        raise ArgumentError("HISQ links and fermion fields must share an element type")
+    for d in dthin_links:
+        if d.gsize != ref.gsize or d.nw != ref.nw or (d.NC1, d.NC2) != (3, 3):
+            raise ArgumentError("HISQ thin-link cotangents must match the links")
+        for u in thin_links:
+            if d is u or d.A.data_ptr() == u.A.data_ptr():
+                raise ArgumentError("HISQ thin-link cotangents must not alias primal links")
+
+
+def hisq_link_pullback_(dthin_links, cache, thin_links, result_cotangent, psi,
+                        coefficient=1.0):
+    """hisq_link_pullback!(dthin_links, cache, thin_links, result_cotangent,
+    psi; coefficient) (HISQPullback.jl:620-699): accumulate into dthin_links
+    the thin-link gradient of coefficient * Re<result_cotangent, D(U) psi>."""
+    _validate_pullback(dthin_links, thin_links, result_cotangent, psi)
+    cache.update_(thin_links)
+    st = _stream()
+    ctx = cache.ctx
+    ctx.set_geometry(psi.gsize, psi.nw, psi.phases, psi.coords, psi.dtype_code)
+    ctx.check(ctx.lib.lmb_hisq_link_pullback(
+        ctx.handle, _ptrs(thin_links), cache.naik_epsilon, float(coefficient),
+        result_cotangent.data_ptr(), psi.data_ptr(), _ptrs(dthin_links), st))
+    for d in dthin_links:
+        mark_halo_dirty_(d)
+    return dthin_links
+
+
+def hisq_fermion_force_(dthin_links, cache, phi, *, rtol=1e-12, atol=0.0,
+                        maxiter=20000, precision="double", delta=0.1):
+    """dS/dU of S = phi^+ (D^+D)^-1 phi for the cached HISQ operator
+    (dSFdU, ext/LatticeMatricesEnzymeExt.jl:387-460): eta = (D^+D)^-1 phi,
+    chi = D eta, force accumulated into dthin_links.  Returns the CGResult."""
+    from ._lib import CG_REASONS, CGParams, CGResultC, PREC
+    from .solver import CGResult
+    thin = cache.thin_links
+    _validate_pullback(dthin_links, thin, phi, phi)
+    prm = CGParams()
+    prm.rtol, prm.atol, prm.maxiter = float(rtol), float(atol), int(maxiter)
+    prm.precision = PREC[precision]
+    prm.delta = float(delta)
+    res = CGResultC()
+    st = _stream()
+    ctx = cache.ctx
+    ctx.set_geometry(phi.gsize, phi.nw, phi.phases, phi.coords, phi.dtype_code)
+    ep = (ctypes.c_uint64 * 4)(*[u.halo_epoch.core for u in thin])
+    ctx.check(ctx.lib.lmb_hisq_fermion_force(
+        ctx.handle, _ptrs(thin), ep, cache.mass, cache.naik_epsilon,
+        phi.data_ptr(), _ptrs(dthin_links), ctypes.byref(prm),
+        ctypes.byref(res), st))
+    for d in dthin_links:
+        mark_halo_dirty_(d)
+    return CGResult(bool(res.converged), res.iterations, res.residual_norm,
+                    res.relative_residual, CG_REASONS[res.reason],
+                    res.reliable_updates, res.true_residual_norm)
