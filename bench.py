@@ -93,6 +93,14 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
+    ap.add_argument("--workload", default="clover",
+                    choices=["clover", "wilson8", "hisq", "batched", "force"],
+                    help="clover: 32^3x64 Wilson-clover mixed vs FP64 CG (the "
+                         "headline line); wilson8: 8^4 Wilson FP64 CG beside the "
+                         "CPU oracle; hisq: 48^3x96 HISQ smearing + CG; batched: "
+                         "multi-RHS multi-lattice Wilson CG; force: 24^4 HISQ "
+                         "fermion force with a finite-difference check")
+    ap.add_argument("--fd-directions", type=int, default=8)
     return ap.parse_args()
 
 
@@ -455,12 +463,214 @@ class _Null:
         return False
 
 
+def _events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _timed(fn, stream):
+    import torch
+    a, b = _events()
+    torch.cuda.synchronize()
+    a.record(stream)
+    out = fn()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return out, a.elapsed_time(b) / 1e3
+
+
+def run_wilson8(args):
+    """Plain Wilson D'D CG, FP64, 8^4, kappa 0.125, links
+    exp(0.3 i H) seed 1, source seed 2; GPU solve and the CPU oracle's full
+    solve on all host cores."""
+    import numpy as np
+    import torch
+    import lmb200 as lmb
+    from oracle import oracle as orc
+    L = (8, 8, 8, 8)
+    U = lmb.random_su3_links(L, 0.3, 1)
+    b = lmb.gaussian_fermion(L, 3, 4, 2, phases=PHASES)
+    D = lmb.WilsonDiracOperator4D(U, 0.125)
+    A = lmb.DdagDOp(D, b.similar())
+    x = b.similar()
+    st = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        lmb.clear_matrix_(x)
+        lmb.cg_(x, A, b, rtol=1e-10)
+    ts = []
+    for _ in range(args.steps):
+        lmb.clear_matrix_(x)
+        res, t = _timed(lambda: lmb.cg_(x, A, b, rtol=1e-10), st)
+        ts.append(t)
+    orc.build()
+    orc.set_num_threads(os.cpu_count() or 1)
+    Uh = orc.random_su3_links(L, 0.3, 1)
+    bh = orc.gaussian_field(L, 3, 4, 2)
+    op = orc.Operator(orc.OP_WILSON, Uh, L, kappa=0.125)
+    t0 = time.perf_counter()
+    xh, rh = orc.cg_ddagd(op, bh, rtol=1e-10)
+    t_cpu = time.perf_counter() - t0
+    err = float(np.linalg.norm(x.gather_matrix() - xh) / np.linalg.norm(xh))
+    print(json.dumps({"workload": "Wilson D'D CG FP64 8^4, kappa 0.125", "gpu_s": statistics.median(ts),
+                      "gpu_iterations": res.iterations, "cpu_s": t_cpu, "cpu_iterations": rh["iterations"],
+                      "cpu_cores": orc.num_threads(), "solution_rel_diff_vs_oracle": err,
+                      "converged": res.converged}), flush=True)
+
+
+def run_hisq(args):
+    """HISQ smearing (fat7+Lepage, U(3), fat7+Naik) on 48^3x96
+    links exp(0.25 i H), then staggered D'D CG at mass 0.01 to 1e-10 with FP32
+    fat/long links and FP64 reliable updates; FP64 CG for comparison."""
+    import torch
+    import lmb200 as lmb
+    L = tuple(int(v) for v in (args.lattice if args.lattice != "32,32,32,64"
+                                else "48,48,48,96").split(","))
+    sites = L[0] * L[1] * L[2] * L[3]
+    U = lmb.random_su3_links(L, 0.25, 1, nw=3)
+    st = torch.cuda.current_stream()
+    links, t_smear = _timed(lambda: lmb.hisq_links_from_thin(U, 0.0), st)
+    links, t_smear = _timed(lambda: lmb.hisq_links_from_thin(U, 0.0), st)
+    D = lmb.HISQDiracOperator4D(links, 0.01, 0.0)
+    b = lmb.gaussian_fermion(L, 3, 1, 2, nw=3, phases=PHASES)
+    A = lmb.DdagDOp(D, b.similar())
+    x = b.similar()
+    out = {"workload": "HISQ smearing + staggered D'D CG, %dx%dx%dx%d, m 0.01" % L,
+           "smear_s": t_smear}
+    for prec in ("single", "double"):
+        lmb.clear_matrix_(x)
+        lmb.cg_(x, A, b, rtol=1e-10, precision=prec, maxiter=args.maxiter)
+        lmb.clear_matrix_(x)
+        res, t = _timed(lambda: lmb.cg_(x, A, b, rtol=1e-10, precision=prec,
+                                         maxiter=args.maxiter, profile=True), st)
+        k1 = res.dslash_ms / max(res.dslash_launches, 1)
+        k2 = res.update_ms / max(res.update_launches, 1)
+        rb = 4 if prec == "single" else 8
+        # each link matrix is read once per site (the backward hops reuse the
+        # neighbours' links): 4 fat + 4 Naik x 18 reals = 144 reals.
+        # K1: links + in + out = 156 reals per site;
+        # K2: links + in + p + r (rw) + x (rw) = 180 reals per site
+        out[prec] = {"time_s": t, "iterations": res.iterations, "converged": res.converged,
+                     "true_rel_residual": res.true_residual_norm / max(1e-300, float(
+                         torch.linalg.vector_norm(b.core_view()))),
+                     "reliable_updates": res.reliable_updates,
+                     "k1_ms": k1, "k1_gbs": 156 * rb * sites / (k1 * 1e-3) / 1e9,
+                     "k2_ms": k2, "k2_gbs": 180 * rb * sites / (k2 * 1e-3) / 1e9}
+    out["speedup_single_vs_fp64"] = out["double"]["time_s"] / out["single"]["time_s"]
+    print(json.dumps(out), flush=True)
+
+
+def run_batched(args):
+    """16 Gaussian right-hand sides of Wilson D'D on 32^4 plus
+    lattices 8^4 x4, 12^4 x4, 16^4 x2, 24^4 x1, in one batched solve (FP32
+    inner, FP64 reliable updates, CUDA graph, autotuned); compared with
+    solving the same systems one right-hand side at a time."""
+    import torch
+    import lmb200 as lmb
+    shapes = [((32, 32, 32, 32), 16), ((8, 8, 8, 8), 4), ((12, 12, 12, 12), 4),
+              ((16, 16, 16, 16), 2), ((24, 24, 24, 24), 1)]
+    systems = []
+    for i, (L, n) in enumerate(shapes):
+        U = lmb.random_su3_links(L, 0.2, 10 + i)
+        D = lmb.WilsonDiracOperator4D(U, 0.12)
+        pairs = []
+        for r in range(n):
+            b = lmb.gaussian_fermion(L, 3, 4, 100 * i + r, phases=PHASES)
+            pairs.append((b.similar(), b))
+        systems.append((D, pairs))
+    st = torch.cuda.current_stream()
+
+    def clear():
+        for _, pairs in systems:
+            for x, _ in pairs:
+                lmb.clear_matrix_(x)
+
+    clear()
+    lmb.cg_batched_(systems, rtol=1e-10)          # tuning + warm-up
+    clear()
+    (res, tune), t_batch = _timed(lambda: lmb.cg_batched_(systems, rtol=1e-10), st)
+    # one right-hand side at a time, same kernels' single-system path
+    def sequential():
+        rs = []
+        for D, pairs in systems:
+            A = lmb.DdagDOp(D, pairs[0][1].similar())
+            for x, b in pairs:
+                rs.append(lmb.cg_(x, A, b, rtol=1e-10, precision="single"))
+        return rs
+    clear()
+    sequential()
+    clear()
+    rs, t_seq = _timed(sequential, st)
+    total_sites_rhs = sum(L[0] * L[1] * L[2] * L[3] * n for L, n in shapes)
+    print(json.dumps({"workload": "batched Wilson D'D CG: 32^4 x16 + 8^4 x4 + 12^4 x4 + 16^4 x2 + 24^4 x1",
+                      "batched_s": t_batch, "sequential_s": t_seq, "speedup": t_seq / t_batch,
+                      "all_converged": all(r.converged for r in res),
+                      "max_iterations": max(r.iterations for r in res),
+                      "tuning": tune, "site_rhs": total_sites_rhs}), flush=True)
+
+
+def run_force(args):
+    """Fermion force dS/dU, S = phi^+ (D^+D)^-1 phi, HISQ smearing
+    on 24^4 (mass 0.02, links exp(0.2 i H)); central finite differences
+    (eps 1e-5) of S along random link directions."""
+    import numpy as np
+    import torch
+    import lmb200 as lmb
+    L = tuple(int(v) for v in (args.lattice if args.lattice != "32,32,32,64"
+                                else "24,24,24,24").split(","))
+    U = lmb.random_su3_links(L, 0.2, 1, nw=3)
+    phi = lmb.gaussian_fermion(L, 3, 1, 2, nw=3, phases=PHASES)
+    cache = lmb.HISQDiracCache4D(U, 0.02, 0.0)
+    dU = [u.similar() for u in U]
+    st = torch.cuda.current_stream()
+    lmb.hisq_fermion_force_(dU, cache, phi, rtol=1e-12)
+    for d in dU:
+        lmb.clear_matrix_(d)
+    res, t_force = _timed(lambda: lmb.hisq_fermion_force_(dU, cache, phi, rtol=1e-12), st)
+    G = [d.core_view().clone() for d in dU]
+    base = [u.core_view().clone() for u in U]
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    h = 1e-5
+    x = phi.similar()
+    def action():
+        c2 = lmb.HISQDiracCache4D(U, 0.02, 0.0)
+        lmb.clear_matrix_(x)
+        r = lmb.cg_(x, lmb.DdagDOp(c2, phi.similar()), phi, rtol=1e-13, maxiter=50000)
+        return lmb.dot(phi, x).real
+    worst = 0.0
+    for k in range(args.fd_directions):
+        V = [torch.randn(b.shape, dtype=b.dtype, device=b.device, generator=gen) for b in base]
+        for s_ in (+1, -1):
+            for u, b, v in zip(U, base, V):
+                u.core_view().copy_(b + s_ * h * v)
+                lmb.mark_halo_dirty_(u)
+            val = action()
+            if s_ > 0:
+                sp = val
+            else:
+                sm = val
+        fd = (sp - sm) / (2 * h)
+        an = sum(float((g.conj() * v).sum().real) for g, v in zip(G, V))
+        worst = max(worst, abs(an - fd) / abs(fd))
+    for u, b in zip(U, base):
+        u.core_view().copy_(b)
+        lmb.mark_halo_dirty_(u)
+    print(json.dumps({"workload": "HISQ fermion force %dx%dx%dx%d m 0.02" % L,
+                      "force_s": t_force, "cg_iterations": res.iterations,
+                      "fd_directions": args.fd_directions, "fd_eps": h,
+                      "max_rel_diff_vs_fd": worst}), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
-    else:
+    elif args.workload == "clover":
         run_lmb(args)
+    else:
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        {"wilson8": run_wilson8, "hisq": run_hisq, "batched": run_batched,
+         "force": run_force}[args.workload](args)
 
 
 if __name__ == "__main__":
