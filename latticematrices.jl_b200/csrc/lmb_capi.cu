@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "lmb_context.cuh"
@@ -162,6 +163,26 @@ int launch_wilson_g(lmb_ctx *ctx, const Field<PS, 12> &in, const G &U, int dagge
                     cudaStream_t st) {
   typedef typename Real<PS>::type R;
   const Geom &g = ctx->g;
+  if constexpr (PS != PREC_DOUBLE) {
+    if (ctx->pair_sites && g.L[3] % 2 == 0) {
+      const unsigned grid2 = grid_for(g.V / 2, kDslashThreads);
+      if constexpr (CLOVER) {
+        const Clover<PG> A = clover_view<PG>(ctx->clover, g.V);
+        if (dagger)
+          wilson_dslash_pair_kernel<1, true><<<grid2, kDslashThreads, 0, st>>>(g, in, U, A, (float)kappa, epi);
+        else
+          wilson_dslash_pair_kernel<0, true><<<grid2, kDslashThreads, 0, st>>>(g, in, U, A, (float)kappa, epi);
+      } else {
+        const NoClover A{g.V};
+        if (dagger)
+          wilson_dslash_pair_kernel<1, false><<<grid2, kDslashThreads, 0, st>>>(g, in, U, A, (float)kappa, epi);
+        else
+          wilson_dslash_pair_kernel<0, false><<<grid2, kDslashThreads, 0, st>>>(g, in, U, A, (float)kappa, epi);
+      }
+      LMB_CHECK_LAUNCH(ctx);
+      return LMB_OK;
+    }
+  }
   const unsigned grid = grid_for(g.V, kDslashThreads);
   if constexpr (CLOVER) {
     const Clover<PG> A = clover_view<PG>(ctx->clover, g.V);
@@ -1274,6 +1295,7 @@ lmb_ctx *lmb_create(int device) {
   if (cudaSetDevice(device) != cudaSuccess) return nullptr;
   lmb_ctx *ctx = new lmb_ctx();
   ctx->device = device;
+  if (const char *ps = getenv("LMB_PAIR_SITES")) ctx->pair_sites = atoi(ps) != 0;
   if (cudaMalloc(&ctx->counter, sizeof(unsigned)) != cudaSuccess ||
       cudaMemset(ctx->counter, 0, sizeof(unsigned)) != cudaSuccess ||
       cudaMalloc(&ctx->st_dev, sizeof(CGState)) != cudaSuccess ||

@@ -82,6 +82,9 @@ struct lmb_ctx {
   lmb::Geom g{};
   lmb::Padded pd{};
   int dtype = LMB_DTYPE_C128;
+  // FP32 / int16 Wilson stencils with two sites per thread (packed FP32);
+  // LMB_PAIR_SITES=0 in the environment selects one site per thread
+  bool pair_sites = true;
   lmb::LinkSet links[3];
   lmb::CloverCache clover;
   std::map<std::string, std::pair<void *, size_t>> buffers;

@@ -124,6 +124,9 @@ struct EpiStore {
   template <typename R> LMB_D void operator()(int s, bool active, const Cx<R> *v) const {
     if (active) out.store(s, v);
   }
+  LMB_D void pair(int s0, int s1, bool active, const Cx2 *v) const {
+    if (active) store2(out, s0, s1, v);
+  }
 };
 
 template <int PS, int NC = 12>
@@ -138,6 +141,18 @@ struct EpiStoreNorm {  // K1
     if (active) {
       out.store(s, v);
       n2[0] = sum_norm2(v, NC);
+    }
+    if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0)
+      finalize_pAp(st, tot[0]);
+  }
+  LMB_D void pair(int s0, int s1, bool active, const Cx2 *v) const {
+    double n2[1] = {0.0}, tot[1];
+    if (active) {
+      store2(out, s0, s1, v);
+      float2 q = f2(0.f);
+#pragma unroll
+      for (int k = 0; k < NC; k++) q = norm2_acc(v[k], q);
+      n2[0] = (double)q.x + (double)q.y;
     }
     if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0)
       finalize_pAp(st, tot[0]);
@@ -168,6 +183,29 @@ struct EpiCGUpdate {  // K2
       r.store(s, rv);
       x.store(s, xv);
       n2[0] = sum_norm2(rv, NC);
+    }
+    if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0)
+      finalize_rr(st, tot[0]);
+  }
+  LMB_D void pair(int s0, int s1, bool active, const Cx2 *v) const {
+    double n2[1] = {0.0}, tot[1];
+    if (active) {
+      const float a = (float)st->alpha;
+      const float2 pa = f2(a), na = f2(-a);
+      Cx2 pv[NC], rv[NC], xv[NC];
+      load2(p, s0, s1, pv);
+      load2(r, s0, s1, rv);
+      load2(x, s0, s1, xv);
+      float2 q = f2(0.f);
+#pragma unroll
+      for (int k = 0; k < NC; k++) {
+        rv[k] = Cx2(fma2(na, v[k].re, rv[k].re), fma2(na, v[k].im, rv[k].im));
+        xv[k] = Cx2(fma2(pa, pv[k].re, xv[k].re), fma2(pa, pv[k].im, xv[k].im));
+        q = norm2_acc(rv[k], q);
+      }
+      store2(r, s0, s1, rv);
+      store2(x, s0, s1, xv);
+      n2[0] = (double)q.x + (double)q.y;
     }
     if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0)
       finalize_rr(st, tot[0]);

@@ -17,6 +17,7 @@
 // components (plain store, store + |out|^2, or a fused CG update).
 #pragma once
 #include "lmb_common.cuh"
+#include "lmb_pair.cuh"
 
 namespace lmb {
 
@@ -27,6 +28,11 @@ namespace lmb {
 #endif
 #ifndef LMB_DSLASH_MINB
 #define LMB_DSLASH_MINB 0
+#endif
+// two-site kernels: 3 resident blocks of 128 threads per SM (<= 168
+// registers) measured fastest on B200
+#ifndef LMB_PAIR_MINB
+#define LMB_PAIR_MINB 3
 #endif
 constexpr int kDslashThreads = LMB_DSLASH_THREADS;
 
@@ -223,6 +229,109 @@ __global__ void __launch_bounds__(kDslashThreads, LMB_DSLASH_MINB)
     }
   }
   epi(s, active, out);
+}
+
+// ---------------------------------------------------------------------------
+// two sites per thread (FP32 arithmetic; see lmb_pair.cuh): lane x = site
+// s0 = (x, y, z, t), lane y = site s1 = s0 + V/2 = (x, y, z, t + T/2), T even.
+// Along x, y, z both lanes step identically (same wrap); along t each lane
+// has its own neighbour and wrap.
+// ---------------------------------------------------------------------------
+// h *= phase on the lanes whose hop crossed the edge
+LMB_D void phase2(Cx2 *h, const double *ph, int w0, int w1) {
+  const float pr = (float)ph[0], pi = (float)ph[1];
+  const Cx2 f(f2(w0 ? pr : 1.f, w1 ? pr : 1.f), f2(w0 ? pi : 0.f, w1 ? pi : 0.f));
+#pragma unroll
+  for (int k = 0; k < 6; k++) h[k] = h[k] * f;
+}
+
+template <int DAG, int MU, class SF, class G>
+LMB_D void hop_dir2(const Geom &g, int s0, const int *c0, int s1, const int *c1, const SF &in, const G &U,
+                    Cx2 *acc) {
+  constexpr int FPM = DAG ? +1 : -1;
+  constexpr int BPM = -FPM;
+  const bool ph = (g.phase_mask >> MU) & 1;
+  Cx2 p[12], h[6], uh[6], u[9];
+  {
+    int w0, w1;
+    const int sp0 = fwd_site(g, s0, c0, MU, 1, &w0);
+    int sp1;
+    if (MU < 3) {
+      sp1 = sp0 + (s1 - s0);
+      w1 = w0;
+    } else {
+      sp1 = fwd_site(g, s1, c1, MU, 1, &w1);
+    }
+    load2(in, sp0, sp1, p);
+    project<FPM, MU>(p, h);
+    if (ph && (w0 | w1)) phase2(h, g.ph_fwd[MU], w0, w1);
+    load2(U, MU, s0, s1, u);
+    su3_mul_half(u, h, uh);
+    reconstruct<FPM, MU>(acc, uh);
+  }
+  {
+    int w0, w1;
+    const int sm0 = bwd_site(g, s0, c0, MU, 1, &w0);
+    int sm1;
+    if (MU < 3) {
+      sm1 = sm0 + (s1 - s0);
+      w1 = w0;
+    } else {
+      sm1 = bwd_site(g, s1, c1, MU, 1, &w1);
+    }
+    load2(in, sm0, sm1, p);
+    project<BPM, MU>(p, h);
+    if (ph && (w0 | w1)) phase2(h, g.ph_bwd[MU], w0, w1);
+    load2(U, MU, sm0, sm1, u);
+    su3_adj_mul_half(u, h, uh);
+    reconstruct<BPM, MU>(acc, uh);
+  }
+}
+
+// The two-site Wilson(-clover) kernel: V/2 threads.  Epi must provide
+// skip() and pair(s0, s1, active, out[12]) with out[k] holding both sites.
+template <int DAG, bool CLOVER, class SF, class G, class CL, class Epi>
+__global__ void __launch_bounds__(kDslashThreads, LMB_PAIR_MINB)
+    wilson_dslash_pair_kernel(const Geom g, const SF in, const G U, const CL A, const float kappa, Epi epi) {
+  if (epi.skip()) return;
+  const int vh = (int)(g.V >> 1);
+  const int s0 = blockIdx.x * kDslashThreads + threadIdx.x;
+  const bool active = s0 < vh;
+  const int s1 = s0 + vh;
+  Cx2 out[12];
+  if (active) {
+    int c0[4], c1[4];
+    site_coords(g, s0, c0);
+    c1[0] = c0[0];
+    c1[1] = c0[1];
+    c1[2] = c0[2];
+    c1[3] = c0[3] + (g.L[3] >> 1);
+    Cx2 acc[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) acc[k] = cx2_zero();
+    hop_dir2<DAG, 0>(g, s0, c0, s1, c1, in, U, acc);
+    hop_dir2<DAG, 1>(g, s0, c0, s1, c1, in, U, acc);
+    hop_dir2<DAG, 2>(g, s0, c0, s1, c1, in, U, acc);
+    hop_dir2<DAG, 3>(g, s0, c0, s1, c1, in, U, acc);
+    Cx2 p[12];
+    load2(in, s0, s1, p);
+    const float2 k2 = f2(kappa);
+    if constexpr (CLOVER) {
+      float2 a[36];
+      Cx2 o[6];
+#pragma unroll
+      for (int blk = 0; blk < 2; blk++) {
+        load2(A, blk, s0, s1, a);
+        herm6_mul(a, p + 6 * blk, o);
+#pragma unroll
+        for (int k = 0; k < 6; k++) out[6 * blk + k] = cfms_real(k2, acc[6 * blk + k], o[k]);
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 12; k++) out[k] = cfms_real(k2, acc[k], p[k]);
+    }
+  }
+  epi.pair(s0, s1, active, out);
 }
 
 }  // namespace lmb
