@@ -158,9 +158,9 @@ template <> Clover<PREC_HALF> clover_view<PREC_HALF>(const CloverCache &cc, int6
 // ---------------------------------------------------------------------------
 // stencil launch
 // ---------------------------------------------------------------------------
-template <int PS, int PG, bool CLOVER, class G, class Epi>
-int launch_wilson_g(lmb_ctx *ctx, const Field<PS, 12> &in, const G &U, int dagger, double kappa, const Epi &epi,
-                    cudaStream_t st) {
+template <int PS, int PG, bool CLOVER, int PHM, class G, class Epi>
+void launch_wilson_phm(lmb_ctx *ctx, const Field<PS, 12> &in, const G &U, int dagger, double kappa,
+                       const Epi &epi, cudaStream_t st) {
   typedef typename Real<PS>::type R;
   const Geom &g = ctx->g;
   if constexpr (PS != PREC_DOUBLE) {
@@ -169,34 +169,42 @@ int launch_wilson_g(lmb_ctx *ctx, const Field<PS, 12> &in, const G &U, int dagge
       if constexpr (CLOVER) {
         const Clover<PG> A = clover_view<PG>(ctx->clover, g.V);
         if (dagger)
-          wilson_dslash_pair_kernel<1, true><<<grid2, kDslashThreads, 0, st>>>(g, in, U, A, (float)kappa, epi);
+          wilson_dslash_pair_kernel<1, true, PHM><<<grid2, kDslashThreads, 0, st>>>(g, in, U, A, (float)kappa, epi);
         else
-          wilson_dslash_pair_kernel<0, true><<<grid2, kDslashThreads, 0, st>>>(g, in, U, A, (float)kappa, epi);
+          wilson_dslash_pair_kernel<0, true, PHM><<<grid2, kDslashThreads, 0, st>>>(g, in, U, A, (float)kappa, epi);
       } else {
         const NoClover A{g.V};
         if (dagger)
-          wilson_dslash_pair_kernel<1, false><<<grid2, kDslashThreads, 0, st>>>(g, in, U, A, (float)kappa, epi);
+          wilson_dslash_pair_kernel<1, false, PHM><<<grid2, kDslashThreads, 0, st>>>(g, in, U, A, (float)kappa, epi);
         else
-          wilson_dslash_pair_kernel<0, false><<<grid2, kDslashThreads, 0, st>>>(g, in, U, A, (float)kappa, epi);
+          wilson_dslash_pair_kernel<0, false, PHM><<<grid2, kDslashThreads, 0, st>>>(g, in, U, A, (float)kappa, epi);
       }
-      LMB_CHECK_LAUNCH(ctx);
-      return LMB_OK;
+      return;
     }
   }
   const unsigned grid = grid_for(g.V, kDslashThreads);
   if constexpr (CLOVER) {
     const Clover<PG> A = clover_view<PG>(ctx->clover, g.V);
     if (dagger)
-      wilson_dslash_kernel<R, 1, true><<<grid, kDslashThreads, 0, st>>>(g, in, U, A, (R)kappa, epi);
+      wilson_dslash_kernel<R, 1, true, PHM><<<grid, kDslashThreads, 0, st>>>(g, in, U, A, (R)kappa, epi);
     else
-      wilson_dslash_kernel<R, 0, true><<<grid, kDslashThreads, 0, st>>>(g, in, U, A, (R)kappa, epi);
+      wilson_dslash_kernel<R, 0, true, PHM><<<grid, kDslashThreads, 0, st>>>(g, in, U, A, (R)kappa, epi);
   } else {
     const NoClover A{g.V};
     if (dagger)
-      wilson_dslash_kernel<R, 1, false><<<grid, kDslashThreads, 0, st>>>(g, in, U, A, (R)kappa, epi);
+      wilson_dslash_kernel<R, 1, false, PHM><<<grid, kDslashThreads, 0, st>>>(g, in, U, A, (R)kappa, epi);
     else
-      wilson_dslash_kernel<R, 0, false><<<grid, kDslashThreads, 0, st>>>(g, in, U, A, (R)kappa, epi);
+      wilson_dslash_kernel<R, 0, false, PHM><<<grid, kDslashThreads, 0, st>>>(g, in, U, A, (R)kappa, epi);
   }
+}
+
+template <int PS, int PG, bool CLOVER, class G, class Epi>
+int launch_wilson_g(lmb_ctx *ctx, const Field<PS, 12> &in, const G &U, int dagger, double kappa, const Epi &epi,
+                    cudaStream_t st) {
+  if (phase_mode_of(ctx->g.phase_mask) == PH_T)
+    launch_wilson_phm<PS, PG, CLOVER, PH_T>(ctx, in, U, dagger, kappa, epi, st);
+  else
+    launch_wilson_phm<PS, PG, CLOVER, PH_ANY>(ctx, in, U, dagger, kappa, epi, st);
   LMB_CHECK_LAUNCH(ctx);
   return LMB_OK;
 }
@@ -258,8 +266,8 @@ struct StaggeredPolicy {
     if (!ctx->links[LMB_LINKS_THIN].valid) return fail(ctx, LMB_ERR_STATE, "gauge links have not been uploaded");
     return ensure_link_precision(ctx, ctx->links[LMB_LINKS_THIN], prec, st);
   }
-  template <int P, class Epi>
-  int launch(lmb_ctx *ctx, const Field<P, 3> &in, int dagger, const Epi &epi, cudaStream_t st) const {
+  template <int P, int PHM, class Epi>
+  void launch_phm(lmb_ctx *ctx, const Field<P, 3> &in, int dagger, const Epi &epi, cudaStream_t st) const {
     typedef typename Real<P>::type R;
     const Geom &g = ctx->g;
     const unsigned grid = grid_for(g.V, kStagThreads);
@@ -268,17 +276,25 @@ struct StaggeredPolicy {
     if (naik) {
       const Gauge<P> X = gauge_view<P>(ctx->links[LMB_LINKS_FAT], g.V);
       const Gauge<P> Lk = gauge_view<P>(ctx->links[LMB_LINKS_LONG], g.V);
-      staggered_dslash_kernel<R, true><<<grid, kStagThreads, 0, st>>>(g, in, X, Lk, (R)mass, fc, lc, epi);
+      staggered_dslash_kernel<R, true, PHM><<<grid, kStagThreads, 0, st>>>(g, in, X, Lk, (R)mass, fc, lc, epi);
     } else {
       const LinkSet &ls = ctx->links[LMB_LINKS_THIN];
       const NoLinks none{g.V};
       if (ls.recon(P))
-        staggered_dslash_kernel<R, false><<<grid, kStagThreads, 0, st>>>(g, in, gauge12_view<P>(ls, g.V), none,
-                                                                          (R)mass, fc, lc, epi);
+        staggered_dslash_kernel<R, false, PHM><<<grid, kStagThreads, 0, st>>>(g, in, gauge12_view<P>(ls, g.V),
+                                                                               none, (R)mass, fc, lc, epi);
       else
-        staggered_dslash_kernel<R, false><<<grid, kStagThreads, 0, st>>>(g, in, gauge_view<P>(ls, g.V), none,
-                                                                          (R)mass, fc, lc, epi);
+        staggered_dslash_kernel<R, false, PHM><<<grid, kStagThreads, 0, st>>>(g, in, gauge_view<P>(ls, g.V),
+                                                                               none, (R)mass, fc, lc, epi);
     }
+  }
+  template <int P, class Epi>
+  int launch(lmb_ctx *ctx, const Field<P, 3> &in, int dagger, const Epi &epi, cudaStream_t st) const {
+    // PH_T needs at most one edge crossing per t hop: T >= 3
+    if (phase_mode_of(ctx->g.phase_mask) == PH_T && ctx->g.L[3] >= 3)
+      launch_phm<P, PH_T>(ctx, in, dagger, epi, st);
+    else
+      launch_phm<P, PH_ANY>(ctx, in, dagger, epi, st);
     LMB_CHECK_LAUNCH(ctx);
     return LMB_OK;
   }

@@ -17,18 +17,18 @@ namespace lmb {
 
 constexpr int kStagThreads = kDslashThreads;  // the epilogue reductions assume it
 
-// neighbour at signed distance d along mu with the number of edge crossings
+// neighbour at signed distance d (|d| <= 3) along mu with the number of
+// edge crossings; three unrolled steps cover every extent (L = 1 included)
+// without a branch
 LMB_D int shift_site_any(const Geom &g, int s, const int *c, int mu, int d, int *wraps) {
   const int L = g.L[mu];
   int raw = c[mu] + d;
   int w = 0;
-  while (raw >= L) {
-    raw -= L;
-    w++;
-  }
-  while (raw < 0) {
-    raw += L;
-    w--;
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    const int up = raw >= L, dn = raw < 0;
+    raw += (dn - up) * L;
+    w += up - dn;
   }
   *wraps = w;
   return s + (raw - c[mu]) * g.stride[mu];
@@ -64,14 +64,25 @@ LMB_D void su3_adj_mul_vec(const Cx<R> *u, const Cx<R> *v, Cx<R> *o) {
   }
 }
 
+// PH_T (only the t phase may differ from 1, T >= 3 so that a hop crosses
+// the edge at most once): multiply every t hop by the selected factor
+template <typename R>
+LMB_D void apply_wrap_sel(const Geom &g, int wraps, Cx<R> *v) {
+  const double *ph = wraps > 0 ? g.ph_fwd[3] : g.ph_bwd[3];
+  const Cx<R> f(wraps ? (R)ph[0] : (R)1, wraps ? (R)ph[1] : (R)0);
+#pragma unroll
+  for (int i = 0; i < 3; i++) v[i] = v[i] * f;
+}
+
 // forward minus backward hop of one direction at distance D, into acc
-template <typename R, int MU, int D, class SF, class G>
+template <typename R, int MU, int D, int PHM, class SF, class G>
 LMB_D void stag_hop(const Geom &g, int s, const int *c, const SF &in, const G &U, R eta, Cx<R> *acc) {
   Cx<R> v[3], u[9], o[3];
   int w;
   const int sp = (D == 1) ? fwd_site(g, s, c, MU, 1, &w) : shift_site_any(g, s, c, MU, D, &w);
   in.load(sp, v);
-  apply_wraps(g, MU, w, v);
+  if constexpr (PHM == PH_ANY) apply_wraps(g, MU, w, v);
+  else if constexpr (MU == 3) apply_wrap_sel(g, w, v);
   U.load(MU, s, u);
   su3_mul_vec(u, v, o);
 #pragma unroll
@@ -80,7 +91,8 @@ LMB_D void stag_hop(const Geom &g, int s, const int *c, const SF &in, const G &U
   const int sm = (D == 1) ? bwd_site(g, s, c, MU, 1, &wb) : shift_site_any(g, s, c, MU, -D, &wb);
   if (D == 1 && wb) wb = -1;
   in.load(sm, v);
-  apply_wraps(g, MU, wb, v);
+  if constexpr (PHM == PH_ANY) apply_wraps(g, MU, wb, v);
+  else if constexpr (MU == 3) apply_wrap_sel(g, wb, v);
   U.load(MU, sm, u);
   su3_adj_mul_vec(u, v, o);
 #pragma unroll
@@ -93,7 +105,7 @@ struct NoLinks {
 };
 
 // Epi as for the Wilson kernel, on 3-component fields
-template <typename R, bool NAIK, class SF, class GF, class GL, class Epi>
+template <typename R, bool NAIK, int PHM, class SF, class GF, class GL, class Epi>
 __global__ void __launch_bounds__(kStagThreads)
     staggered_dslash_kernel(const Geom g, const SF in, const GF X, const GL Lk, const R mass, const R fc,
                             const R lc, Epi epi) {
@@ -107,18 +119,18 @@ __global__ void __launch_bounds__(kStagThreads)
     const int p0 = c[0] + g.eta_off[0], p1 = p0 + c[1] + g.eta_off[1], p2 = p1 + c[2] + g.eta_off[2];
     const R eta[4] = {(R)1, (p0 & 1) ? (R)-1 : (R)1, (p1 & 1) ? (R)-1 : (R)1, (p2 & 1) ? (R)-1 : (R)1};
     Cx<R> fat[3] = {Cx<R>(0, 0), Cx<R>(0, 0), Cx<R>(0, 0)};
-    stag_hop<R, 0, 1>(g, s, c, in, X, eta[0], fat);
-    stag_hop<R, 1, 1>(g, s, c, in, X, eta[1], fat);
-    stag_hop<R, 2, 1>(g, s, c, in, X, eta[2], fat);
-    stag_hop<R, 3, 1>(g, s, c, in, X, eta[3], fat);
+    stag_hop<R, 0, 1, PHM>(g, s, c, in, X, eta[0], fat);
+    stag_hop<R, 1, 1, PHM>(g, s, c, in, X, eta[1], fat);
+    stag_hop<R, 2, 1, PHM>(g, s, c, in, X, eta[2], fat);
+    stag_hop<R, 3, 1, PHM>(g, s, c, in, X, eta[3], fat);
     Cx<R> psi[3];
     in.load(s, psi);
     if constexpr (NAIK) {
       Cx<R> lng[3] = {Cx<R>(0, 0), Cx<R>(0, 0), Cx<R>(0, 0)};
-      stag_hop<R, 0, 3>(g, s, c, in, Lk, eta[0], lng);
-      stag_hop<R, 1, 3>(g, s, c, in, Lk, eta[1], lng);
-      stag_hop<R, 2, 3>(g, s, c, in, Lk, eta[2], lng);
-      stag_hop<R, 3, 3>(g, s, c, in, Lk, eta[3], lng);
+      stag_hop<R, 0, 3, PHM>(g, s, c, in, Lk, eta[0], lng);
+      stag_hop<R, 1, 3, PHM>(g, s, c, in, Lk, eta[1], lng);
+      stag_hop<R, 2, 3, PHM>(g, s, c, in, Lk, eta[2], lng);
+      stag_hop<R, 3, 3, PHM>(g, s, c, in, Lk, eta[3], lng);
 #pragma unroll
       for (int i = 0; i < 3; i++) out[i] = mass * psi[i] + fc * fat[i] + lc * lng[i];
     } else {

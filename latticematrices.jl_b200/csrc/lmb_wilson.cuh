@@ -118,6 +118,22 @@ LMB_D void scale_phase(Cx<R> *h, int n, const double *ph) {
     if (k < n) h[k] = h[k] * f;
 }
 
+// Boundary-phase code of the stencils.  PH_T: only the t phase may differ
+// from 1 (the usual antiperiodic fermions), applied to every t hop as a
+// multiplication by a selected factor (1 off the edge): no branch, so the
+// compiler is free to issue the next hop's loads early.  PH_ANY: any
+// direction, applied only when the hop crossed the edge.
+enum PhaseMode { PH_T = 0, PH_ANY = 1 };
+
+LMB_HD int phase_mode_of(int phase_mask) { return (phase_mask & ~8) ? PH_ANY : PH_T; }
+
+template <typename R>
+LMB_D void scale_phase_sel(Cx<R> *h, const double *ph, int wrap) {
+  const Cx<R> f(wrap ? (R)ph[0] : (R)1, wrap ? (R)ph[1] : (R)0);
+#pragma unroll
+  for (int k = 0; k < 6; k++) h[k] = h[k] * f;
+}
+
 // Hermitian 6x6 (packed: 6 real diagonal, 15 complex lower triangle in row
 // order) times a 6-vector
 template <typename R>
@@ -137,7 +153,7 @@ LMB_D void herm6_mul(const R *a, const Cx<R> *v, Cx<R> *o) {
 }
 
 // hopping term of one direction, forward and backward, accumulated into acc
-template <typename R, int DAG, int MU, class SF, class G>
+template <typename R, int DAG, int MU, int PHM = PH_ANY, class SF, class G>
 LMB_D void hop_dir(const Geom &g, int s, const int *c, const SF &in, const G &U,
                    Cx<R> *acc) {
   // D: forward (1 - g), backward (1 + g);  D^+: swapped
@@ -149,7 +165,11 @@ LMB_D void hop_dir(const Geom &g, int s, const int *c, const SF &in, const G &U,
     const int sp = fwd_site(g, s, c, MU, 1, &wrap);
     in.load(sp, p);
     project<FPM, MU>(p, h);
-    if (wrap && ((g.phase_mask >> MU) & 1)) scale_phase(h, 6, g.ph_fwd[MU]);
+    if constexpr (PHM == PH_ANY) {
+      if (wrap && ((g.phase_mask >> MU) & 1)) scale_phase(h, 6, g.ph_fwd[MU]);
+    } else if constexpr (MU == 3) {
+      scale_phase_sel(h, g.ph_fwd[3], wrap);
+    }
     U.load(MU, s, u);
     su3_mul_half(u, h, uh);
     reconstruct<FPM, MU>(acc, uh);
@@ -158,7 +178,11 @@ LMB_D void hop_dir(const Geom &g, int s, const int *c, const SF &in, const G &U,
     const int sm = bwd_site(g, s, c, MU, 1, &wrap);
     in.load(sm, p);
     project<BPM, MU>(p, h);
-    if (wrap && ((g.phase_mask >> MU) & 1)) scale_phase(h, 6, g.ph_bwd[MU]);
+    if constexpr (PHM == PH_ANY) {
+      if (wrap && ((g.phase_mask >> MU) & 1)) scale_phase(h, 6, g.ph_bwd[MU]);
+    } else if constexpr (MU == 3) {
+      scale_phase_sel(h, g.ph_bwd[3], wrap);
+    }
     U.load(MU, sm, u);
     su3_adj_mul_half(u, h, uh);
     reconstruct<BPM, MU>(acc, uh);
@@ -191,7 +215,7 @@ LMB_D void wilson_site(const Geom &g, int s, const SF &in, const G &U, R kappa, 
 // The Wilson(-clover) kernel.  Epi must provide:
 //   bool skip() const                      -- whole grid exits (paused solve)
 //   void operator()(s, active, out[12])    -- consume the result
-template <typename R, int DAG, bool CLOVER, class SF, class G, class CL, class Epi>
+template <typename R, int DAG, bool CLOVER, int PHM, class SF, class G, class CL, class Epi>
 __global__ void __launch_bounds__(kDslashThreads, LMB_DSLASH_MINB)
     wilson_dslash_kernel(const Geom g, const SF in, const G U, const CL A,
                          const R kappa, Epi epi) {
@@ -205,10 +229,10 @@ __global__ void __launch_bounds__(kDslashThreads, LMB_DSLASH_MINB)
     Cx<R> acc[12];
 #pragma unroll
     for (int k = 0; k < 12; k++) acc[k] = Cx<R>(0, 0);
-    hop_dir<R, DAG, 0>(g, s, c, in, U, acc);
-    hop_dir<R, DAG, 1>(g, s, c, in, U, acc);
-    hop_dir<R, DAG, 2>(g, s, c, in, U, acc);
-    hop_dir<R, DAG, 3>(g, s, c, in, U, acc);
+    hop_dir<R, DAG, 0, PHM>(g, s, c, in, U, acc);
+    hop_dir<R, DAG, 1, PHM>(g, s, c, in, U, acc);
+    hop_dir<R, DAG, 2, PHM>(g, s, c, in, U, acc);
+    hop_dir<R, DAG, 3, PHM>(g, s, c, in, U, acc);
     Cx<R> p[12];
     in.load(s, p);
     if constexpr (CLOVER) {
@@ -245,7 +269,7 @@ LMB_D void phase2(Cx2 *h, const double *ph, int w0, int w1) {
   for (int k = 0; k < 6; k++) h[k] = h[k] * f;
 }
 
-template <int DAG, int MU, class SF, class G>
+template <int DAG, int MU, int PHM, class SF, class G>
 LMB_D void hop_dir2(const Geom &g, int s0, const int *c0, int s1, const int *c1, const SF &in, const G &U,
                     Cx2 *acc) {
   constexpr int FPM = DAG ? +1 : -1;
@@ -264,7 +288,11 @@ LMB_D void hop_dir2(const Geom &g, int s0, const int *c0, int s1, const int *c1,
     }
     load2(in, sp0, sp1, p);
     project<FPM, MU>(p, h);
-    if (ph && (w0 | w1)) phase2(h, g.ph_fwd[MU], w0, w1);
+    if constexpr (PHM == PH_ANY) {
+      if (ph && (w0 | w1)) phase2(h, g.ph_fwd[MU], w0, w1);
+    } else if constexpr (MU == 3) {
+      phase2(h, g.ph_fwd[3], w0, w1);
+    }
     load2(U, MU, s0, s1, u);
     su3_mul_half(u, h, uh);
     reconstruct<FPM, MU>(acc, uh);
@@ -281,7 +309,11 @@ LMB_D void hop_dir2(const Geom &g, int s0, const int *c0, int s1, const int *c1,
     }
     load2(in, sm0, sm1, p);
     project<BPM, MU>(p, h);
-    if (ph && (w0 | w1)) phase2(h, g.ph_bwd[MU], w0, w1);
+    if constexpr (PHM == PH_ANY) {
+      if (ph && (w0 | w1)) phase2(h, g.ph_bwd[MU], w0, w1);
+    } else if constexpr (MU == 3) {
+      phase2(h, g.ph_bwd[3], w0, w1);
+    }
     load2(U, MU, sm0, sm1, u);
     su3_adj_mul_half(u, h, uh);
     reconstruct<BPM, MU>(acc, uh);
@@ -290,7 +322,7 @@ LMB_D void hop_dir2(const Geom &g, int s0, const int *c0, int s1, const int *c1,
 
 // The two-site Wilson(-clover) kernel: V/2 threads.  Epi must provide
 // skip() and pair(s0, s1, active, out[12]) with out[k] holding both sites.
-template <int DAG, bool CLOVER, class SF, class G, class CL, class Epi>
+template <int DAG, bool CLOVER, int PHM, class SF, class G, class CL, class Epi>
 __global__ void __launch_bounds__(kDslashThreads, LMB_PAIR_MINB)
     wilson_dslash_pair_kernel(const Geom g, const SF in, const G U, const CL A, const float kappa, Epi epi) {
   if (epi.skip()) return;
@@ -309,10 +341,10 @@ __global__ void __launch_bounds__(kDslashThreads, LMB_PAIR_MINB)
     Cx2 acc[12];
 #pragma unroll
     for (int k = 0; k < 12; k++) acc[k] = cx2_zero();
-    hop_dir2<DAG, 0>(g, s0, c0, s1, c1, in, U, acc);
-    hop_dir2<DAG, 1>(g, s0, c0, s1, c1, in, U, acc);
-    hop_dir2<DAG, 2>(g, s0, c0, s1, c1, in, U, acc);
-    hop_dir2<DAG, 3>(g, s0, c0, s1, c1, in, U, acc);
+    hop_dir2<DAG, 0, PHM>(g, s0, c0, s1, c1, in, U, acc);
+    hop_dir2<DAG, 1, PHM>(g, s0, c0, s1, c1, in, U, acc);
+    hop_dir2<DAG, 2, PHM>(g, s0, c0, s1, c1, in, U, acc);
+    hop_dir2<DAG, 3, PHM>(g, s0, c0, s1, c1, in, U, acc);
     Cx2 p[12];
     load2(in, s0, s1, p);
     const float2 k2 = f2(kappa);
