@@ -17,18 +17,20 @@ namespace lmb {
 
 constexpr int kStagThreads = kDslashThreads;  // the epilogue reductions assume it
 
-// neighbour at signed distance d (|d| <= 3) along mu with the number of
-// edge crossings; three unrolled steps cover every extent (L = 1 included)
-// without a branch
+// neighbour at signed distance d along mu with the number of edge crossings
+// (the loops run at most once on extents >= 3; measured faster on B200 than
+// an unrolled branch-free form)
 LMB_D int shift_site_any(const Geom &g, int s, const int *c, int mu, int d, int *wraps) {
   const int L = g.L[mu];
   int raw = c[mu] + d;
   int w = 0;
-#pragma unroll
-  for (int i = 0; i < 3; i++) {
-    const int up = raw >= L, dn = raw < 0;
-    raw += (dn - up) * L;
-    w += up - dn;
+  while (raw >= L) {
+    raw -= L;
+    w++;
+  }
+  while (raw < 0) {
+    raw += L;
+    w--;
   }
   *wraps = w;
   return s + (raw - c[mu]) * g.stride[mu];
