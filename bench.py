@@ -100,7 +100,7 @@ def parse():
                          "CPU oracle; hisq: 48^3x96 HISQ smearing + CG; batched: "
                          "multi-RHS multi-lattice Wilson CG; force: 24^4 HISQ "
                          "fermion force with a finite-difference check")
-    ap.add_argument("--fd-directions", type=int, default=8)
+    ap.add_argument("--fd-directions", type=int, default=64)
     return ap.parse_args()
 
 
@@ -333,6 +333,7 @@ def run_lmb(args):
     t_mixed = max_over_ranks(t_mixed, ws, dev)
     mixed_true = true_rel()
     mixed = results[-1]
+    x_mixed = x.core_view().clone()
 
     # ---- timed: plain FP64 CG (the reference's arithmetic) ----
     r64 = []
@@ -347,6 +348,10 @@ def run_lmb(args):
     t_fp64 = max_over_ranks(start.elapsed_time(end) / 1e3 / args.fp64_steps, ws, dev)
     fp64_true = true_rel()
     res64 = r64[-1]
+    # error of the mixed-precision solution against the FP64 solve
+    mixed_vs_fp64 = float(torch.linalg.vector_norm(x_mixed - x.core_view())
+                          / torch.linalg.vector_norm(x.core_view()))
+    del x_mixed
 
     # ---- e2e: host buffers, copies inside the timed region ----
     b_host = b.A.cpu().pin_memory()
@@ -411,7 +416,8 @@ def run_lmb(args):
         },
         "mixed": {"time_s": t_mixed, "iterations": mixed.iterations,
                   "reliable_updates": mixed.reliable_updates,
-                  "true_rel_residual": mixed_true},
+                  "true_rel_residual": mixed_true,
+                  "solution_rel_diff_vs_fp64": mixed_vs_fp64},
         "fp64": {"time_s": t_fp64, "iterations": res64.iterations,
                  "true_rel_residual": fp64_true},
         "speedup_mixed_vs_fp64": t_fp64 / t_mixed,
