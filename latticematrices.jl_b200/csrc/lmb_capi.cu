@@ -290,9 +290,11 @@ struct StaggeredPolicy {
   }
   template <int P, class Epi>
   int launch(lmb_ctx *ctx, const Field<P, 3> &in, int dagger, const Epi &epi, cudaStream_t st) const {
-    // PH_T needs at most one edge crossing per t hop: T >= 3.  The FP64
-    // HISQ stencils measured faster on B200 with the branch form (PH_ANY).
-    if (P != PREC_DOUBLE && phase_mode_of(ctx->g.phase_mask) == PH_T && ctx->g.L[3] >= 3)
+    // PH_T needs at most one edge crossing per hop: every extent >= 3.  The
+    // FP64 HISQ stencils measured faster on B200 with the branch form (PH_ANY).
+    const int *L = ctx->g.L;
+    if (P != PREC_DOUBLE && phase_mode_of(ctx->g.phase_mask) == PH_T && L[0] >= 3 && L[1] >= 3 && L[2] >= 3 &&
+        L[3] >= 3)
       launch_phm<P, PH_T>(ctx, in, dagger, epi, st);
     else
       launch_phm<P, PH_ANY>(ctx, in, dagger, epi, st);

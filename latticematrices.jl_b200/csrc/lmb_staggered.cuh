@@ -66,6 +66,20 @@ LMB_D void su3_adj_mul_vec(const Cx<R> *u, const Cx<R> *v, Cx<R> *o) {
   }
 }
 
+// neighbour at +d / -d (d <= 3) on an extent >= d: at most one crossing,
+// selected without a branch (the form of fwd_site / bwd_site)
+LMB_D int shift_site_sel(const Geom &g, int s, const int *c, int mu, int d, int *wraps) {
+  const int L = g.L[mu];
+  if (d > 0) {
+    const int up = c[mu] + d >= L;
+    *wraps = up;
+    return s + (up ? d - L : d) * g.stride[mu];
+  }
+  const int dn = c[mu] + d < 0;
+  *wraps = -dn;
+  return s + (dn ? d + L : d) * g.stride[mu];
+}
+
 // PH_T (only the t phase may differ from 1, T >= 3 so that a hop crosses
 // the edge at most once): multiply every t hop by the selected factor
 template <typename R>
@@ -81,7 +95,10 @@ template <typename R, int MU, int D, int PHM, class SF, class G>
 LMB_D void stag_hop(const Geom &g, int s, const int *c, const SF &in, const G &U, R eta, Cx<R> *acc) {
   Cx<R> v[3], u[9], o[3];
   int w;
-  const int sp = (D == 1) ? fwd_site(g, s, c, MU, 1, &w) : shift_site_any(g, s, c, MU, D, &w);
+  // PH_T launches only on extents >= 3: at most one crossing per hop
+  const int sp = (D == 1)          ? fwd_site(g, s, c, MU, 1, &w)
+                 : (PHM == PH_ANY) ? shift_site_any(g, s, c, MU, D, &w)
+                                   : shift_site_sel(g, s, c, MU, D, &w);
   in.load(sp, v);
   if constexpr (PHM == PH_ANY) apply_wraps(g, MU, w, v);
   else if constexpr (MU == 3) apply_wrap_sel(g, w, v);
@@ -90,7 +107,9 @@ LMB_D void stag_hop(const Geom &g, int s, const int *c, const SF &in, const G &U
 #pragma unroll
   for (int i = 0; i < 3; i++) acc[i] = acc[i] + eta * o[i];
   int wb;
-  const int sm = (D == 1) ? bwd_site(g, s, c, MU, 1, &wb) : shift_site_any(g, s, c, MU, -D, &wb);
+  const int sm = (D == 1)          ? bwd_site(g, s, c, MU, 1, &wb)
+                 : (PHM == PH_ANY) ? shift_site_any(g, s, c, MU, -D, &wb)
+                                   : shift_site_sel(g, s, c, MU, -D, &wb);
   if (D == 1 && wb) wb = -1;
   in.load(sm, v);
   if constexpr (PHM == PH_ANY) apply_wraps(g, MU, wb, v);
