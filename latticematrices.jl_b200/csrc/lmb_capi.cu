@@ -53,7 +53,7 @@ int ensure_link_precision(lmb_ctx *ctx, LinkSet &ls, int prec, cudaStream_t st, 
   }
   if (prec == PREC_SINGLE && ls.f_version != ls.version) {
     if (!ls.f) LMB_CUDA(ctx, cudaMalloc(&ls.f, sizeof(float2) * n));
-    links_to_single_kernel<<<grid_for(n, 256), 256, 0, st>>>(ls.f, ls.d, n);
+    links_to_single_kernel<<<grid_for(V, 256), 256, 0, st>>>((float4 *)ls.f, ls.d, V);
     LMB_CHECK_LAUNCH(ctx);
     ls.f_version = ls.version;
   }
@@ -87,7 +87,9 @@ template <> Gauge12<PREC_HALF> gauge12_view<PREC_HALF>(const LinkSet &ls, int64_
 
 template <int P> Gauge<P> gauge_view(const LinkSet &ls, int64_t V);
 template <> Gauge<PREC_DOUBLE> gauge_view<PREC_DOUBLE>(const LinkSet &ls, int64_t V) { return {ls.d, V, ls.scale}; }
-template <> Gauge<PREC_SINGLE> gauge_view<PREC_SINGLE>(const LinkSet &ls, int64_t V) { return {ls.f, V, ls.scale}; }
+template <> Gauge<PREC_SINGLE> gauge_view<PREC_SINGLE>(const LinkSet &ls, int64_t V) {
+  return {(const float4 *)ls.f, V, ls.scale};
+}
 template <> Gauge<PREC_HALF> gauge_view<PREC_HALF>(const LinkSet &ls, int64_t V) {
   return {ls.h, V, base_of_exponent(pow2_exponent(ls.scale))};
 }

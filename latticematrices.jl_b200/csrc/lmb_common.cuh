@@ -276,17 +276,24 @@ template <> struct Gauge<PREC_DOUBLE> {
     }
   }
 };
+// FP32, 18 reals: per direction four float4 planes (entries 2k, 2k+1) and one
+// float2 plane (entry 8) -- five loads per link; data points at the 16 float4
+// planes (mu*4 + k), followed by the 4 float2 planes (mu) at data + 16 V
 template <> struct Gauge<PREC_SINGLE> {
-  const float2 *data;
+  const float4 *data;
   int64_t V;
   float scale;
   static size_t bytes(int64_t V) { return sizeof(float2) * 36 * V; }
+  LMB_D const float2 *last() const { return reinterpret_cast<const float2 *>(data + 16 * V); }
   template <typename R> LMB_D void load(int mu, int64_t s, Cx<R> *u) const {
 #pragma unroll
-    for (int k = 0; k < 9; k++) {
-      float2 t = __ldg(data + (mu * 9 + k) * V + s);
-      u[k] = Cx<R>((R)t.x, (R)t.y);
+    for (int k = 0; k < 4; k++) {
+      const float4 t = __ldg(data + (mu * 4 + k) * V + s);
+      u[2 * k] = Cx<R>((R)t.x, (R)t.y);
+      u[2 * k + 1] = Cx<R>((R)t.z, (R)t.w);
     }
+    const float2 t = __ldg(last() + mu * V + s);
+    u[8] = Cx<R>((R)t.x, (R)t.y);
   }
 };
 template <> struct Gauge<PREC_HALF> {

@@ -76,11 +76,20 @@ __global__ void __launch_bounds__(256)
 
 // 36 double2 link planes -> single / half copies
 __global__ void __launch_bounds__(256)
-    links_to_single_kernel(float2 *dst, const double2 *src, int64_t n) {
-  const int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x;
-  if (i >= n) return;
-  const double2 t = src[i];
-  dst[i] = make_float2((float)t.x, (float)t.y);
+    links_to_single_kernel(float4 *dst, const double2 *src, int64_t V) {
+  // 36 double2 planes (mu*9 + e) -> Gauge<PREC_SINGLE>: float4 planes
+  // (mu*4 + k) holding entries 2k, 2k+1, then float2 planes (mu) holding 8
+  const int64_t s = (int64_t)blockIdx.x * 256 + threadIdx.x;
+  if (s >= V) return;
+  float2 *last = reinterpret_cast<float2 *>(dst + 16 * V);
+  for (int mu = 0; mu < 4; mu++) {
+    for (int k = 0; k < 4; k++) {
+      const double2 a = src[(mu * 9 + 2 * k) * V + s], b = src[(mu * 9 + 2 * k + 1) * V + s];
+      dst[(mu * 4 + k) * V + s] = make_float4((float)a.x, (float)a.y, (float)b.x, (float)b.y);
+    }
+    const double2 c = src[(mu * 9 + 8) * V + s];
+    last[mu * V + s] = make_float2((float)c.x, (float)c.y);
+  }
 }
 
 // k = scale exponent (|values| <= 2^k)

@@ -203,10 +203,13 @@ LMB_D void store2(const Field<PREC_SINGLE, NC> &f, int64_t s0, int64_t s1, const
 // links: 18 reals
 LMB_D void load2(const Gauge<PREC_SINGLE> &U, int mu, int64_t s0, int64_t s1, Cx2 *u) {
 #pragma unroll
-  for (int k = 0; k < 9; k++) {
-    const float2 a = __ldg(U.data + (mu * 9 + k) * U.V + s0), b = __ldg(U.data + (mu * 9 + k) * U.V + s1);
-    u[k] = Cx2(f2(a.x, b.x), f2(a.y, b.y));
+  for (int k = 0; k < 4; k++) {
+    const float4 a = __ldg(U.data + (mu * 4 + k) * U.V + s0), b = __ldg(U.data + (mu * 4 + k) * U.V + s1);
+    u[2 * k] = Cx2(f2(a.x, b.x), f2(a.y, b.y));
+    u[2 * k + 1] = Cx2(f2(a.z, b.z), f2(a.w, b.w));
   }
+  const float2 a = __ldg(U.last() + mu * U.V + s0), b = __ldg(U.last() + mu * U.V + s1);
+  u[8] = Cx2(f2(a.x, b.x), f2(a.y, b.y));
 }
 LMB_D void load2(const Gauge<PREC_HALF> &U, int mu, int64_t s0, int64_t s1, Cx2 *u) {
   const unsigned y = __float_as_uint(U.scale) >> 16;
