@@ -154,24 +154,26 @@ template <int NCOMP> struct Field<PREC_SINGLE, NCOMP> {
   }
 };
 
-// three-component (staggered) FP32 field: three float2 planes, no padding
+// three-component (staggered) FP32 field, no padding: one float4 plane
+// (components 0, 1) followed by one float2 plane (component 2) -- two loads
 template <> struct Field<PREC_SINGLE, 3> {
-  float2 *data;
+  float4 *data;
   float *norm;
   int64_t V;
-  static constexpr int kPlanes = 3;
+  static constexpr int kPlanes = 2;
   static size_t bytes(int64_t V) { return sizeof(float2) * 3 * V; }
   static size_t norm_bytes(int64_t) { return 0; }
+  LMB_D float2 *last() const { return reinterpret_cast<float2 *>(data + V); }
   template <typename R> LMB_D void load(int64_t s, Cx<R> *v) const {
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-      const float2 t = __ldg(data + k * V + s);
-      v[k] = Cx<R>((R)t.x, (R)t.y);
-    }
+    const float4 a = __ldg(data + s);
+    const float2 b = __ldg(last() + s);
+    v[0] = Cx<R>((R)a.x, (R)a.y);
+    v[1] = Cx<R>((R)a.z, (R)a.w);
+    v[2] = Cx<R>((R)b.x, (R)b.y);
   }
   template <typename R> LMB_D void store(int64_t s, const Cx<R> *v) const {
-#pragma unroll
-    for (int k = 0; k < 3; k++) data[k * V + s] = make_float2((float)v[k].re, (float)v[k].im);
+    data[s] = make_float4((float)v[0].re, (float)v[0].im, (float)v[1].re, (float)v[1].im);
+    last()[s] = make_float2((float)v[2].re, (float)v[2].im);
   }
 };
 
