@@ -165,6 +165,25 @@ void launch_wilson_phm(lmb_ctx *ctx, const Field<PS, 12> &in, const G &U, int da
                        const Epi &epi, cudaStream_t st) {
   typedef typename Real<PS>::type R;
   const Geom &g = ctx->g;
+  if constexpr (PS == PREC_HALF && std::is_same<G, Gauge12<PREC_HALF>>::value) {
+    if (ctx->pair_sites && ctx->adj_sites && g.L[0] % 2 == 0) {
+      const unsigned grid2 = grid_for(g.V / 2, kDslashThreads);
+      if constexpr (CLOVER) {
+        const Clover<PG> A = clover_view<PG>(ctx->clover, g.V);
+        if (dagger)
+          wilson_half_adj_kernel<1, true, PHM><<<grid2, kDslashThreads, 0, st>>>(g, in, U, A, (float)kappa, epi);
+        else
+          wilson_half_adj_kernel<0, true, PHM><<<grid2, kDslashThreads, 0, st>>>(g, in, U, A, (float)kappa, epi);
+      } else {
+        const NoClover A{g.V};
+        if (dagger)
+          wilson_half_adj_kernel<1, false, PHM><<<grid2, kDslashThreads, 0, st>>>(g, in, U, A, (float)kappa, epi);
+        else
+          wilson_half_adj_kernel<0, false, PHM><<<grid2, kDslashThreads, 0, st>>>(g, in, U, A, (float)kappa, epi);
+      }
+      return;
+    }
+  }
   if constexpr (PS != PREC_DOUBLE) {
     if (ctx->pair_sites && g.L[3] % 2 == 0) {
       const unsigned grid2 = grid_for(g.V / 2, kDslashThreads);
@@ -1317,6 +1336,7 @@ lmb_ctx *lmb_create(int device) {
   lmb_ctx *ctx = new lmb_ctx();
   ctx->device = device;
   if (const char *ps = getenv("LMB_PAIR_SITES")) ctx->pair_sites = atoi(ps) != 0;
+  if (const char *as = getenv("LMB_ADJ_SITES")) ctx->adj_sites = atoi(as) != 0;
   if (cudaMalloc(&ctx->counter, sizeof(unsigned)) != cudaSuccess ||
       cudaMemset(ctx->counter, 0, sizeof(unsigned)) != cudaSuccess ||
       cudaMalloc(&ctx->st_dev, sizeof(CGState)) != cudaSuccess ||

@@ -85,6 +85,10 @@ struct lmb_ctx {
   // FP32 / int16 Wilson stencils with two sites per thread (packed FP32);
   // LMB_PAIR_SITES=0 in the environment selects one site per thread
   bool pair_sites = true;
+  // int16 Wilson stencils with reconstruct-12 links and an even x extent:
+  // the two sites of a thread are x-neighbours, read with 256-bit loads
+  // (environment LMB_ADJ_SITES=0: sites s and s + V/2)
+  bool adj_sites = true;
   lmb::LinkSet links[3];
   lmb::CloverCache clover;
   std::map<std::string, std::pair<void *, size_t>> buffers;

@@ -276,6 +276,71 @@ LMB_D void load2(const Clover<PREC_HALF> &A, int blk, int64_t s0, int64_t s1, fl
   a[35] = v1.im;
 }
 
+// ---------------------------------------------------------------------------
+// adjacent pairs: lanes are sites s and s + 1 (s even).  One 256-bit load
+// (sm_100 ld.global.v8) fetches a plane's 16-byte words of both sites; the
+// address must be 32-byte aligned, which holds for even s on planes of an
+// even number of sites.
+// ---------------------------------------------------------------------------
+LMB_D void ld256(const int4 *p, int4 &a, int4 &b) {
+  asm("ld.global.nc.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
+      : "l"(p));
+}
+
+template <int NC>
+LMB_D void load_adj(const Field<PREC_HALF, NC> &f, int64_t s, Cx2 *v) {
+  const float2 nb = __ldg(reinterpret_cast<const float2 *>(f.norm + s));
+  const unsigned y0 = __float_as_uint(nb.x) >> 16, y1 = __float_as_uint(nb.y) >> 16;
+  const float2 negc = make_float2(-nb.x * 1.00390625f, -nb.y * 1.00390625f);
+  constexpr int P = Field<PREC_HALF, NC>::kPlanes;
+#pragma unroll
+  for (int k = 0; k < P; k++) {
+    int4 t0, t1;
+    ld256(f.data + k * f.V + s, t0, t1);
+    const int w0[4] = {t0.x, t0.y, t0.z, t0.w}, w1[4] = {t1.x, t1.y, t1.z, t1.w};
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      if (4 * k + j < NC) v[4 * k + j] = dec_pair2(w0[j], w1[j], y0, y1, negc);
+  }
+}
+LMB_D void load_adj(const Gauge12<PREC_HALF> &U, int mu, int64_t s, Cx2 *u) {
+  const int q0 = mu * 6, p0 = q0 >> 2, lane0 = q0 & 3;
+  int4 a0, a1, b0, b1;
+  ld256(U.data + p0 * U.V + s, a0, a1);
+  ld256(U.data + (p0 + 1) * U.V + s, b0, b1);
+  const int w0[8] = {a0.x, a0.y, a0.z, a0.w, b0.x, b0.y, b0.z, b0.w};
+  const int w1[8] = {a1.x, a1.y, a1.z, a1.w, b1.x, b1.y, b1.z, b1.w};
+  const float2 negc = f2(-257.0f);  // base 2^8
+#pragma unroll
+  for (int e = 0; e < 6; e++)
+    u[(e / 3) + 3 * (e % 3)] = dec_pair2(w0[lane0 + e], w1[lane0 + e], 0x4380u, 0x4380u, negc);
+  su3_third_row(u);
+}
+LMB_D void load_adj(const Clover<PREC_HALF> &A, int blk, int64_t s, float2 *a) {
+  const unsigned y = __float_as_uint(A.scale) >> 16;
+  const float2 negc = f2(-A.scale * 1.00390625f);
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    int4 t0, t1;
+    ld256(A.data + (blk * 4 + k) * A.V + s, t0, t1);
+    const int w0[4] = {t0.x, t0.y, t0.z, t0.w}, w1[4] = {t1.x, t1.y, t1.z, t1.w};
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const Cx2 v = dec_pair2(w0[j], w1[j], y, y, negc);
+      a[8 * k + 2 * j] = v.re;
+      a[8 * k + 2 * j + 1] = v.im;
+    }
+  }
+  // the two sites' int2 tails are one 16-byte word
+  const int4 t = __ldg(reinterpret_cast<const int4 *>(A.tail + blk * A.V + s));
+  const Cx2 v0 = dec_pair2(t.x, t.z, y, y, negc), v1 = dec_pair2(t.y, t.w, y, y, negc);
+  a[32] = v0.re;
+  a[33] = v0.im;
+  a[34] = v1.re;
+  a[35] = v1.im;
+}
+
 // Hermitian 6x6 (6 real diagonal, 15 complex lower entries) times a 6-vector
 LMB_D void herm6_mul(const float2 *a, const Cx2 *v, Cx2 *o) {
 #pragma unroll

@@ -366,4 +366,110 @@ __global__ void __launch_bounds__(kDslashThreads, LMB_PAIR_MINB)
   epi.pair(s0, s1, active, out);
 }
 
+// ---------------------------------------------------------------------------
+// int16 storage, reconstruct-12 links: lanes are x-adjacent sites s0 = 2i
+// (x even) and s1 = s0 + 1 (lmb_pair.cuh: one 256-bit load per plane serves
+// both).  y, z, t hops and the site's own links, spinor and clover use those
+// loads; x hops, whose neighbours differ per lane, load each lane.
+// ---------------------------------------------------------------------------
+template <int DAG, int MU, int PHM>
+LMB_D void hop_adj(const Geom &g, int s0, const int *c0, const int *c1, const Field<PREC_HALF, 12> &in,
+                   const Gauge12<PREC_HALF> &U, Cx2 *acc) {
+  constexpr int FPM = DAG ? +1 : -1;
+  constexpr int BPM = -FPM;
+  const bool ph = (g.phase_mask >> MU) & 1;
+  Cx2 p[12], h[6], uh[6], u[9];
+  {
+    int w0, w1;
+    if constexpr (MU == 0) {
+      w0 = 0;  // x + 1 of an even x never crosses the edge
+      const int n1 = fwd_site(g, s0 + 1, c1, 0, 1, &w1);
+      load2(in, s0 + 1, n1, p);
+    } else {
+      load_adj(in, fwd_site(g, s0, c0, MU, 1, &w0), p);
+      w1 = w0;
+    }
+    project<FPM, MU>(p, h);
+    if constexpr (PHM == PH_ANY) {
+      if (ph && (w0 | w1)) phase2(h, g.ph_fwd[MU], w0, w1);
+    } else if constexpr (MU == 3) {
+      phase2(h, g.ph_fwd[3], w0, w1);
+    }
+    load_adj(U, MU, s0, u);
+    su3_mul_half(u, h, uh);
+    reconstruct<FPM, MU>(acc, uh);
+  }
+  {
+    int w0, w1;
+    if constexpr (MU == 0) {
+      const int n0 = bwd_site(g, s0, c0, 0, 1, &w0);
+      w1 = 0;  // x - 1 of an odd x never crosses the edge
+      load2(in, n0, s0, p);
+      project<BPM, MU>(p, h);
+      if constexpr (PHM == PH_ANY) {
+        if (ph && (w0 | w1)) phase2(h, g.ph_bwd[MU], w0, w1);
+      }
+      load2(U, 0, n0, s0, u);
+    } else {
+      const int n0 = bwd_site(g, s0, c0, MU, 1, &w0);
+      w1 = w0;
+      load_adj(in, n0, p);
+      project<BPM, MU>(p, h);
+      if constexpr (PHM == PH_ANY) {
+        if (ph && (w0 | w1)) phase2(h, g.ph_bwd[MU], w0, w1);
+      } else if constexpr (MU == 3) {
+        phase2(h, g.ph_bwd[3], w0, w1);
+      }
+      load_adj(U, MU, n0, u);
+    }
+    su3_adj_mul_half(u, h, uh);
+    reconstruct<BPM, MU>(acc, uh);
+  }
+}
+
+// V/2 threads; needs x even.  Epi as for wilson_dslash_pair_kernel.
+template <int DAG, bool CLOVER, int PHM, class CL, class Epi>
+__global__ void __launch_bounds__(kDslashThreads, LMB_PAIR_MINB)
+    wilson_half_adj_kernel(const Geom g, const Field<PREC_HALF, 12> in, const Gauge12<PREC_HALF> U, const CL A,
+                           const float kappa, Epi epi) {
+  if (epi.skip()) return;
+  const int i = blockIdx.x * kDslashThreads + threadIdx.x;
+  const bool active = i < (int)(g.V >> 1);
+  const int s0 = 2 * i;
+  Cx2 out[12];
+  if (active) {
+    int c0[4], c1[4];
+    site_coords(g, s0, c0);
+    c1[0] = c0[0] + 1;
+    c1[1] = c0[1];
+    c1[2] = c0[2];
+    c1[3] = c0[3];
+    Cx2 acc[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) acc[k] = cx2_zero();
+    hop_adj<DAG, 0, PHM>(g, s0, c0, c1, in, U, acc);
+    hop_adj<DAG, 1, PHM>(g, s0, c0, c1, in, U, acc);
+    hop_adj<DAG, 2, PHM>(g, s0, c0, c1, in, U, acc);
+    hop_adj<DAG, 3, PHM>(g, s0, c0, c1, in, U, acc);
+    Cx2 p[12];
+    load_adj(in, s0, p);
+    const float2 k2 = f2(kappa);
+    if constexpr (CLOVER) {
+      float2 a[36];
+      Cx2 o[6];
+#pragma unroll
+      for (int blk = 0; blk < 2; blk++) {
+        load_adj(A, blk, s0, a);
+        herm6_mul(a, p + 6 * blk, o);
+#pragma unroll
+        for (int k = 0; k < 6; k++) out[6 * blk + k] = cfms_real(k2, acc[6 * blk + k], o[k]);
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 12; k++) out[k] = cfms_real(k2, acc[k], p[k]);
+    }
+  }
+  epi.pair(s0, s0 + 1, active, out);
+}
+
 }  // namespace lmb

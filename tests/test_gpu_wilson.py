@@ -83,13 +83,18 @@ def test_complex64_fields(lmb, orc):
 
 @pytest.mark.parametrize("precision,tol", [("single", 5e-6), ("half", 2e-3)])
 @pytest.mark.parametrize("clover", [False, True])
-@pytest.mark.parametrize("L,pair", [((8, 4, 4, 8), "1"), ((8, 4, 4, 8), "0"),
-                                    ((6, 4, 4, 2), "1"), ((4, 6, 4, 5), "1")])
-def test_low_precision_storage(lmb, orc, precision, tol, clover, L, pair, monkeypatch):
-    """Even T runs two sites per thread (s and s + V/2, packed FP32) unless
-    LMB_PAIR_SITES=0; odd T always runs one site per thread.  T = 2 puts
-    every t-hop of one of the two lanes across the boundary."""
+@pytest.mark.parametrize("L,pair,adj", [((8, 4, 4, 8), "1", "1"), ((8, 4, 4, 8), "1", "0"),
+                                        ((8, 4, 4, 8), "0", "1"), ((6, 4, 4, 2), "1", "1"),
+                                        ((6, 4, 4, 2), "1", "0"), ((4, 6, 4, 5), "1", "1"),
+                                        ((5, 4, 4, 6), "1", "1"), ((5, 3, 4, 5), "1", "1")])
+def test_low_precision_storage(lmb, orc, precision, tol, clover, L, pair, adj, monkeypatch):
+    """Two sites per thread in packed FP32 unless LMB_PAIR_SITES=0: int16
+    storage with an even x extent pairs x-neighbours (256-bit loads) unless
+    LMB_ADJ_SITES=0; otherwise an even T pairs s and s + V/2 (T = 2 puts every
+    t-hop of one lane across the boundary); odd x and T run one site per
+    thread."""
     monkeypatch.setenv("LMB_PAIR_SITES", pair)
+    monkeypatch.setenv("LMB_ADJ_SITES", adj)
     U, psi, Ud, pd = _fields(lmb, orc, L, phases=TWISTED)
     D = lmb.WilsonDiracCloverOperator4D(Ud, 0.1355, 1.0) if clover \
         else lmb.WilsonDiracOperator4D(Ud, 0.1355)
