@@ -288,6 +288,92 @@ LMB_D void ld256(const int4 *p, int4 &a, int4 &b) {
       : "l"(p));
 }
 
+LMB_D void st256(int4 *p, const int4 &a, const int4 &b) {
+  asm volatile("st.global.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "r"(a.x), "r"(a.y), "r"(a.z),
+               "r"(a.w), "r"(b.x), "r"(b.y), "r"(b.z), "r"(b.w)
+               : "memory");
+}
+// 256-bit load of data this kernel also writes (no read-only cache path)
+LMB_D void ld256_rw(const int4 *p, int4 &a, int4 &b) {
+  asm volatile("ld.global.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
+               : "l"(p)
+               : "memory");
+}
+
+// own-site fields of the epilogues (read and written by the same kernel)
+template <int NC>
+LMB_D void load_adj_rw(const Field<PREC_HALF, NC> &f, int64_t s, Cx2 *v) {
+  const float2 nb = *reinterpret_cast<const float2 *>(f.norm + s);
+  const unsigned y0 = __float_as_uint(nb.x) >> 16, y1 = __float_as_uint(nb.y) >> 16;
+  const float2 negc = make_float2(-nb.x * 1.00390625f, -nb.y * 1.00390625f);
+  constexpr int P = Field<PREC_HALF, NC>::kPlanes;
+#pragma unroll
+  for (int k = 0; k < P; k++) {
+    int4 t0, t1;
+    ld256_rw(f.data + k * f.V + s, t0, t1);
+    const int w0[4] = {t0.x, t0.y, t0.z, t0.w}, w1[4] = {t1.x, t1.y, t1.z, t1.w};
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      if (4 * k + j < NC) v[4 * k + j] = dec_pair2(w0[j], w1[j], y0, y1, negc);
+  }
+}
+template <int NC>
+LMB_D void load_adj_rw(const Field<PREC_SINGLE, NC> &f, int64_t s, Cx2 *v) {
+  constexpr int P = Field<PREC_SINGLE, NC>::kPlanes;
+#pragma unroll
+  for (int k = 0; k < P; k++) {
+    int4 ia, ib;
+    ld256_rw(reinterpret_cast<const int4 *>(f.data + k * f.V + s), ia, ib);
+    const float4 a = *reinterpret_cast<const float4 *>(&ia), b = *reinterpret_cast<const float4 *>(&ib);
+    v[2 * k] = Cx2(f2(a.x, b.x), f2(a.y, b.y));
+    if (2 * k + 1 < NC) v[2 * k + 1] = Cx2(f2(a.z, b.z), f2(a.w, b.w));
+  }
+}
+template <int NC>
+LMB_D void store_adj(const Field<PREC_HALF, NC> &f, int64_t s, const Cx2 *v) {
+  float m0 = 0.f, m1 = 0.f;
+#pragma unroll
+  for (int k = 0; k < NC; k++) {
+    m0 = fmaxf(m0, fmaxf(fabsf(v[k].re.x), fabsf(v[k].im.x)));
+    m1 = fmaxf(m1, fmaxf(fabsf(v[k].re.y), fabsf(v[k].im.y)));
+  }
+  const int e0 = enc_exponent(m0), e1 = enc_exponent(m1);
+  const float2 inv = make_float2(enc_inv(e0), enc_inv(e1));
+  const float2 mag = f2(8421376.0f);  // 2^23 + 2^15
+  constexpr int P = Field<PREC_HALF, NC>::kPlanes;
+#pragma unroll
+  for (int k = 0; k < P; k++) {
+    int w0[4], w1[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      if (4 * k + j < NC) {
+        const float2 qr = fma2(v[4 * k + j].re, inv, mag), qi = fma2(v[4 * k + j].im, inv, mag);
+        w0[j] = enc_word(qr.x, qi.x);
+        w1[j] = enc_word(qr.y, qi.y);
+      } else {
+        w0[j] = w1[j] = (int)0x80008000u;  // q = 0
+      }
+    }
+    st256(f.data + k * f.V + s, make_int4(w0[0], w0[1], w0[2], w0[3]), make_int4(w1[0], w1[1], w1[2], w1[3]));
+  }
+  *reinterpret_cast<float2 *>(f.norm + s) = make_float2(enc_base(e0), enc_base(e1));
+}
+template <int NC>
+LMB_D void store_adj(const Field<PREC_SINGLE, NC> &f, int64_t s, const Cx2 *v) {
+  constexpr int P = Field<PREC_SINGLE, NC>::kPlanes;
+#pragma unroll
+  for (int k = 0; k < P; k++) {
+    const bool two = 2 * k + 1 < NC;
+    const float4 a = make_float4(v[2 * k].re.x, v[2 * k].im.x, two ? v[2 * k + 1].re.x : 0.f,
+                                 two ? v[2 * k + 1].im.x : 0.f);
+    const float4 b = make_float4(v[2 * k].re.y, v[2 * k].im.y, two ? v[2 * k + 1].re.y : 0.f,
+                                 two ? v[2 * k + 1].im.y : 0.f);
+    st256(reinterpret_cast<int4 *>(f.data + k * f.V + s), *reinterpret_cast<const int4 *>(&a),
+          *reinterpret_cast<const int4 *>(&b));
+  }
+}
+
 template <int NC>
 LMB_D void load_adj(const Field<PREC_HALF, NC> &f, int64_t s, Cx2 *v) {
   const float2 nb = __ldg(reinterpret_cast<const float2 *>(f.norm + s));

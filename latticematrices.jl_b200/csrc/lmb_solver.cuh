@@ -127,6 +127,10 @@ struct EpiStore {
   LMB_D void pair(int s0, int s1, bool active, const Cx2 *v) const {
     if (active) store2(out, s0, s1, v);
   }
+  // s0 even, s1 = s0 + 1
+  LMB_D void pair_adj(int s0, bool active, const Cx2 *v) const {
+    if (active) store_adj(out, s0, v);
+  }
 };
 
 template <int PS, int NC = 12>
@@ -141,6 +145,18 @@ struct EpiStoreNorm {  // K1
     if (active) {
       out.store(s, v);
       n2[0] = sum_norm2(v, NC);
+    }
+    if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0)
+      finalize_pAp(st, tot[0]);
+  }
+  LMB_D void pair_adj(int s0, bool active, const Cx2 *v) const {
+    double n2[1] = {0.0}, tot[1];
+    if (active) {
+      store_adj(out, s0, v);
+      float2 q = f2(0.f);
+#pragma unroll
+      for (int k = 0; k < NC; k++) q = norm2_acc(v[k], q);
+      n2[0] = (double)q.x + (double)q.y;
     }
     if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0)
       finalize_pAp(st, tot[0]);
@@ -183,6 +199,29 @@ struct EpiCGUpdate {  // K2
       r.store(s, rv);
       x.store(s, xv);
       n2[0] = sum_norm2(rv, NC);
+    }
+    if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0)
+      finalize_rr(st, tot[0]);
+  }
+  LMB_D void pair_adj(int s0, bool active, const Cx2 *v) const {
+    double n2[1] = {0.0}, tot[1];
+    if (active) {
+      const float a = (float)st->alpha;
+      const float2 pa = f2(a), na = f2(-a);
+      Cx2 pv[NC], rv[NC], xv[NC];
+      load_adj_rw(p, s0, pv);
+      load_adj_rw(r, s0, rv);
+      load_adj_rw(x, s0, xv);
+      float2 q = f2(0.f);
+#pragma unroll
+      for (int k = 0; k < NC; k++) {
+        rv[k] = Cx2(fma2(na, v[k].re, rv[k].re), fma2(na, v[k].im, rv[k].im));
+        xv[k] = Cx2(fma2(pa, pv[k].re, xv[k].re), fma2(pa, pv[k].im, xv[k].im));
+        q = norm2_acc(rv[k], q);
+      }
+      store_adj(r, s0, rv);
+      store_adj(x, s0, xv);
+      n2[0] = (double)q.x + (double)q.y;
     }
     if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0)
       finalize_rr(st, tot[0]);

@@ -427,7 +427,8 @@ LMB_D void hop_adj(const Geom &g, int s0, const int *c0, const int *c1, const Fi
   }
 }
 
-// V/2 threads; needs x even.  Epi as for wilson_dslash_pair_kernel.
+// V/2 threads; needs x even.  Epi must provide skip() and
+// pair_adj(s0, active, out[12]) (sites s0 and s0 + 1).
 template <int DAG, bool CLOVER, int PHM, class CL, class Epi>
 __global__ void __launch_bounds__(kDslashThreads, LMB_PAIR_MINB)
     wilson_half_adj_kernel(const Geom g, const Field<PREC_HALF, 12> in, const Gauge12<PREC_HALF> U, const CL A,
@@ -469,7 +470,7 @@ __global__ void __launch_bounds__(kDslashThreads, LMB_PAIR_MINB)
       for (int k = 0; k < 12; k++) out[k] = cfms_real(k2, acc[k], p[k]);
     }
   }
-  epi.pair(s0, s0 + 1, active, out);
+  epi.pair_adj(s0, active, out);
 }
 
 }  // namespace lmb
