@@ -402,6 +402,19 @@ int read_state(lmb_ctx *ctx, cudaStream_t st) {
 }
 
 // PS: precision of the iterated fields (DOUBLE = plain FP64 CG), PX: of x_low
+// K3: p = r + beta p; FP32 / int16 Wilson fields of an even volume use the
+// two-site kernel (256-bit accesses)
+template <int PS, int NC>
+void launch_p_update(lmb_ctx *ctx, Field<PS, NC> &p, const Field<PS, NC> &r, int64_t V, cudaStream_t st) {
+  if constexpr (PS != PREC_DOUBLE && NC == 12) {
+    if (ctx->pair_sites && ctx->adj_sites && V % 2 == 0) {
+      cg_p_update_adj_kernel<PS><<<grid_for(V / 2, kBlasThreads), kBlasThreads, 0, st>>>(p, r, ctx->st_dev, V);
+      return;
+    }
+  }
+  cg_p_update_kernel<PS, NC><<<grid_for(V, kBlasThreads), kBlasThreads, 0, st>>>(p, r, ctx->st_dev, V);
+}
+
 template <int PS, int PX, class Op>
 int cg_run(lmb_ctx *ctx, const lmb_cg_params *prm, const Op &op, void *x_pad, const void *b_pad,
            lmb_cg_result *res, cudaStream_t st) {
@@ -496,7 +509,7 @@ int cg_run(lmb_ctx *ctx, const lmb_cg_params *prm, const Op &op, void *x_pad, co
       if (rc) return rc;
       nl++;
       if (prm->profile) cudaEventRecord(pool.ev[4 * i + 2], st);
-      cg_p_update_kernel<PS, NC><<<bgrid, kBlasThreads, 0, st>>>(p, rl, ctx->st_dev, V);
+      launch_p_update<PS, NC>(ctx, p, rl, V, st);
       LMB_CHECK_LAUNCH(ctx);
       nl++;
       if (prm->profile) cudaEventRecord(pool.ev[4 * i + 3], st);
@@ -523,7 +536,7 @@ int cg_run(lmb_ctx *ctx, const lmb_cg_params *prm, const Op &op, void *x_pad, co
         // resume: the true-residual kernel runs regardless of the pause
         rc = true_residual(1);
         if (rc) return rc;
-        cg_p_update_kernel<PS, NC><<<bgrid, kBlasThreads, 0, st>>>(p, rl, ctx->st_dev, V);
+        launch_p_update<PS, NC>(ctx, p, rl, V, st);
         LMB_CHECK_LAUNCH(ctx);
         nl++;
         rc = read_state(ctx, st);

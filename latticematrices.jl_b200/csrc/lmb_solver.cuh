@@ -300,6 +300,23 @@ __global__ void __launch_bounds__(kBlasThreads)
   p.store(s, pv);
 }
 
+// K3 on x-adjacent site pairs (V even; FP32 or int16 storage, NC = 12):
+// packed FP32 and 256-bit loads / stores, V/2 threads
+template <int PS>
+__global__ void __launch_bounds__(kBlasThreads)
+    cg_p_update_adj_kernel(Field<PS, 12> p, const Field<PS, 12> r, const CGState *st, int64_t V) {
+  if (((volatile const CGState *)st)->status != ST_RUNNING) return;
+  const int64_t s = 2 * ((int64_t)blockIdx.x * kBlasThreads + threadIdx.x);
+  if (s >= V) return;
+  const float2 beta = f2((float)st->beta);
+  Cx2 pv[12], rv[12];
+  load_adj_rw(p, s, pv);
+  load_adj_rw(r, s, rv);
+#pragma unroll
+  for (int k = 0; k < 12; k++) pv[k] = Cx2(fma2(beta, pv[k].re, rv[k].re), fma2(beta, pv[k].im, rv[k].im));
+  store_adj(p, s, pv);
+}
+
 // dst = src (precision conversion)
 template <int PD, int PSRC, int NC>
 __global__ void __launch_bounds__(kBlasThreads)
