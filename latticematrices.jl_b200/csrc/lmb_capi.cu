@@ -401,7 +401,6 @@ int read_state(lmb_ctx *ctx, cudaStream_t st) {
   return LMB_OK;
 }
 
-// PS: precision of the iterated fields (DOUBLE = plain FP64 CG), PX: of x_low
 // K3: p = r + beta p; FP32 / int16 Wilson fields of an even volume use the
 // two-site kernel (256-bit accesses)
 template <int PS, int NC>
@@ -415,6 +414,7 @@ void launch_p_update(lmb_ctx *ctx, Field<PS, NC> &p, const Field<PS, NC> &r, int
   cg_p_update_kernel<PS, NC><<<grid_for(V, kBlasThreads), kBlasThreads, 0, st>>>(p, r, ctx->st_dev, V);
 }
 
+// PS: precision of the iterated fields (DOUBLE = plain FP64 CG), PX: of x_low
 template <int PS, int PX, class Op>
 int cg_run(lmb_ctx *ctx, const lmb_cg_params *prm, const Op &op, void *x_pad, const void *b_pad,
            lmb_cg_result *res, cudaStream_t st) {
@@ -439,7 +439,7 @@ int cg_run(lmb_ctx *ctx, const lmb_cg_params *prm, const Op &op, void *x_pad, co
     xl = *(Field<PX, NC> *)&x64;
   }
   const unsigned dgrid = grid_for(V, kDslashThreads), bgrid = grid_for(V, kBlasThreads);
-  if (!ensure_partials(ctx, dgrid > bgrid ? dgrid : bgrid, 1))
+  if (!ensure_partials(ctx, dgrid > bgrid ? dgrid : bgrid, 2))
     return fail(ctx, LMB_ERR_CUDA, "out of device memory (reduction partials)");
   rc = op.prepare(ctx, PREC_DOUBLE, st);
   if (rc) return rc;
@@ -463,10 +463,13 @@ int cg_run(lmb_ctx *ctx, const lmb_cg_params *prm, const Op &op, void *x_pad, co
     LMB_CUDA(ctx, cudaMemsetAsync(xl.data, 0, Field<PX, NC>::bytes(V), st));
     if (xl.norm) LMB_CUDA(ctx, cudaMemsetAsync(xl.norm, 0, Field<PX, NC>::norm_bytes(V), st));
   }
-  norm_b_kernel<NC><<<bgrid, kBlasThreads, 0, st>>>(b64, ctx->st_dev, V, prm->rtol, prm->atol, ctx->partials,
-                                                     ctx->counter);
+  norm_bx_kernel<NC><<<bgrid, kBlasThreads, 0, st>>>(b64, x64, ctx->st_dev, V, prm->rtol, prm->atol,
+                                                      ctx->partials, ctx->counter);
   LMB_CHECK_LAUNCH(ctx);
   nl++;
+  rc = read_state(ctx, st);
+  if (rc) return rc;
+  const bool zero_guess = ctx->st_host->xx == 0.0;
   // r = b - D'D x (FP64)
   auto true_residual = [&](int mode) -> int {
     EpiStore<PREC_DOUBLE, NC> e1{t64, nullptr};
@@ -476,8 +479,16 @@ int cg_run(lmb_ctx *ctx, const lmb_cg_params *prm, const Op &op, void *x_pad, co
     EpiTrueResidual<PS, NC> e2{b64, r64, rl, mixed ? 1 : 0, mode, ctx->st_dev, ctx->partials, ctx->counter};
     return op.template launch<PREC_DOUBLE>(ctx, t64, 1, e2, st);
   };
-  rc = true_residual(0);
-  if (rc) return rc;
+  if (zero_guess) {
+    // b - D'D 0 = b exactly: one pass instead of two FP64 stencils
+    residual_of_zero_kernel<PS, NC><<<dgrid, kDslashThreads, 0, st>>>(b64, r64, rl, mixed ? 1 : 0, 0, ctx->st_dev,
+                                                                      V, ctx->partials, ctx->counter);
+    LMB_CHECK_LAUNCH(ctx);
+    nl++;
+  } else {
+    rc = true_residual(0);
+    if (rc) return rc;
+  }
   convert_kernel<PS, PS, NC><<<bgrid, kBlasThreads, 0, st>>>(p, rl, V);
   LMB_CHECK_LAUNCH(ctx);
   nl++;

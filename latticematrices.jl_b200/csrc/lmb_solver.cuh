@@ -43,6 +43,7 @@ struct CGState {
   double rr_true;   // last FP64 true residual |b - D^+D x|^2
   double rr_pending;
   double bb;
+  double xx;        // |x0|^2 of the initial guess
   int iter;
   int maxiter;
   int status;
@@ -351,6 +352,50 @@ __global__ void __launch_bounds__(kBlasThreads)
   }
   x.store(s, a);
   xl.store(s, z);
+}
+
+// |b|^2 into st->bb and the tolerance, |x0|^2 into st->xx
+template <int NC>
+__global__ void __launch_bounds__(kBlasThreads)
+    norm_bx_kernel(const Field<PREC_DOUBLE, NC> b, const Field<PREC_DOUBLE, NC> x, CGState *st, int64_t V,
+                   double rtol, double atol, double *partials, unsigned *counter) {
+  const int64_t s = (int64_t)blockIdx.x * kBlasThreads + threadIdx.x;
+  double n2[2] = {0.0, 0.0}, tot[2];
+  if (s < V) {
+    Cx<double> v[NC];
+    b.load(s, v);
+#pragma unroll
+    for (int k = 0; k < NC; k++) n2[0] += norm2(v[k]);
+    x.load(s, v);
+#pragma unroll
+    for (int k = 0; k < NC; k++) n2[1] += norm2(v[k]);
+  }
+  if (grid_reduce<kBlasThreads, 2>(n2, partials, counter, tot) && threadIdx.x == 0) {
+    st->bb = tot[0];
+    st->xx = tot[1];
+    const double bn = sqrt(tot[0]);
+    const double tol = fmax(atol, rtol * bn);
+    st->tol2 = tol * tol;
+  }
+}
+
+// the initial residual of a zero guess: r = b, r_low = r (optional),
+// |r|^2 -> finalize_true(mode); blocks of kDslashThreads sites, the partition
+// of the stencil epilogue it replaces (same reduction order)
+template <int PS, int NC>
+__global__ void __launch_bounds__(kDslashThreads)
+    residual_of_zero_kernel(const Field<PREC_DOUBLE, NC> b, Field<PREC_DOUBLE, NC> r, Field<PS, NC> r_low,
+                            int write_low, int mode, CGState *st, int64_t V, double *partials, unsigned *counter) {
+  const int64_t s = (int64_t)blockIdx.x * kDslashThreads + threadIdx.x;
+  double n2[1] = {0.0}, tot[1];
+  if (s < V) {
+    Cx<double> v[NC];
+    b.load(s, v);
+    r.store(s, v);
+    if (write_low) r_low.store(s, v);
+    n2[0] = sum_norm2(v, NC);
+  }
+  if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0) finalize_true(st, tot[0], mode);
 }
 
 // |a|^2 into st->bb and the tolerance
