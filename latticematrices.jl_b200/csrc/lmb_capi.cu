@@ -294,6 +294,22 @@ struct StaggeredPolicy {
     const unsigned grid = grid_for(g.V, kStagThreads);
     const R fc = (R)(dagger ? -0.5 : 0.5);
     const R lc = (R)(dagger ? (1.0 + eps) / 48.0 : -(1.0 + eps) / 48.0);
+    if constexpr (P == PREC_SINGLE && PHM == PH_T) {
+      // x-adjacent two-site kernel: even x extent, 18-real FP32 links
+      const LinkSet &thin = ctx->links[LMB_LINKS_THIN];
+      if (ctx->pair_sites && ctx->adj_sites && g.L[0] % 2 == 0 && (naik || !thin.recon(P))) {
+        const unsigned grid2 = grid_for(g.V / 2, kStagThreads);
+        if (naik) {
+          const Gauge<P> X = gauge_view<P>(ctx->links[LMB_LINKS_FAT], g.V);
+          const Gauge<P> Lk = gauge_view<P>(ctx->links[LMB_LINKS_LONG], g.V);
+          staggered_adj_kernel<true><<<grid2, kStagThreads, 0, st>>>(g, in, X, Lk, mass, fc, lc, epi);
+        } else {
+          const Gauge<P> X = gauge_view<P>(thin, g.V);
+          staggered_adj_kernel<false><<<grid2, kStagThreads, 0, st>>>(g, in, X, X, mass, fc, lc, epi);
+        }
+        return;
+      }
+    }
     if (naik) {
       const Gauge<P> X = gauge_view<P>(ctx->links[LMB_LINKS_FAT], g.V);
       const Gauge<P> Lk = gauge_view<P>(ctx->links[LMB_LINKS_LONG], g.V);

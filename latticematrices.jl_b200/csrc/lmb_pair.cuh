@@ -427,6 +427,55 @@ LMB_D void load_adj(const Clover<PREC_HALF> &A, int blk, int64_t s, float2 *a) {
   a[35] = v1.im;
 }
 
+// 3-component FP32 fields (float4 plane + float2 plane) and 18-real FP32
+// links (four float4 planes + one float2 plane per direction), adjacent pairs
+LMB_D float4 as_f4(const int4 &v) { return make_float4(__int_as_float(v.x), __int_as_float(v.y), __int_as_float(v.z), __int_as_float(v.w)); }
+LMB_D int4 as_i4(const float4 &v) { return make_int4(__float_as_int(v.x), __float_as_int(v.y), __float_as_int(v.z), __float_as_int(v.w)); }
+
+LMB_D void load_adj(const Field<PREC_SINGLE, 3> &f, int64_t s, Cx2 *v) {
+  int4 ia, ib;
+  ld256(reinterpret_cast<const int4 *>(f.data + s), ia, ib);
+  const float4 a = as_f4(ia), b = as_f4(ib);
+  const float4 c = __ldg(reinterpret_cast<const float4 *>(f.last() + s));  // (s).xy, (s + 1).xy
+  v[0] = Cx2(f2(a.x, b.x), f2(a.y, b.y));
+  v[1] = Cx2(f2(a.z, b.z), f2(a.w, b.w));
+  v[2] = Cx2(f2(c.x, c.z), f2(c.y, c.w));
+}
+LMB_D void load_adj_rw(const Field<PREC_SINGLE, 3> &f, int64_t s, Cx2 *v) {
+  int4 ia, ib;
+  ld256_rw(reinterpret_cast<const int4 *>(f.data + s), ia, ib);
+  const float4 a = as_f4(ia), b = as_f4(ib);
+  const float4 c = *reinterpret_cast<const float4 *>(f.last() + s);
+  v[0] = Cx2(f2(a.x, b.x), f2(a.y, b.y));
+  v[1] = Cx2(f2(a.z, b.z), f2(a.w, b.w));
+  v[2] = Cx2(f2(c.x, c.z), f2(c.y, c.w));
+}
+LMB_D void store_adj(const Field<PREC_SINGLE, 3> &f, int64_t s, const Cx2 *v) {
+  st256(reinterpret_cast<int4 *>(f.data + s), as_i4(make_float4(v[0].re.x, v[0].im.x, v[1].re.x, v[1].im.x)),
+        as_i4(make_float4(v[0].re.y, v[0].im.y, v[1].re.y, v[1].im.y)));
+  *reinterpret_cast<float4 *>(f.last() + s) = make_float4(v[2].re.x, v[2].im.x, v[2].re.y, v[2].im.y);
+}
+// two arbitrary sites
+LMB_D void load2(const Field<PREC_SINGLE, 3> &f, int64_t s0, int64_t s1, Cx2 *v) {
+  const float4 a = __ldg(f.data + s0), b = __ldg(f.data + s1);
+  const float2 c = __ldg(f.last() + s0), d = __ldg(f.last() + s1);
+  v[0] = Cx2(f2(a.x, b.x), f2(a.y, b.y));
+  v[1] = Cx2(f2(a.z, b.z), f2(a.w, b.w));
+  v[2] = Cx2(f2(c.x, d.x), f2(c.y, d.y));
+}
+LMB_D void load_adj(const Gauge<PREC_SINGLE> &U, int mu, int64_t s, Cx2 *u) {
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    int4 ia, ib;
+    ld256(reinterpret_cast<const int4 *>(U.data + (mu * 4 + k) * U.V + s), ia, ib);
+    const float4 a = as_f4(ia), b = as_f4(ib);
+    u[2 * k] = Cx2(f2(a.x, b.x), f2(a.y, b.y));
+    u[2 * k + 1] = Cx2(f2(a.z, b.z), f2(a.w, b.w));
+  }
+  const float4 c = __ldg(reinterpret_cast<const float4 *>(U.last() + mu * U.V + s));
+  u[8] = Cx2(f2(c.x, c.z), f2(c.y, c.w));
+}
+
 // Hermitian 6x6 (6 real diagonal, 15 complex lower entries) times a 6-vector
 LMB_D void herm6_mul(const float2 *a, const Cx2 *v, Cx2 *o) {
 #pragma unroll

@@ -162,4 +162,113 @@ __global__ void __launch_bounds__(kStagThreads)
   epi(s, active, out);
 }
 
+// ---------------------------------------------------------------------------
+// FP32 HISQ / staggered stencil on x-adjacent site pairs (s0 = 2i, s1 = s0 + 1)
+// with packed FP32 arithmetic and 256-bit loads (lmb_pair.cuh).  Conditions
+// of the PH_T mode (only the t phase, every extent >= 3) and an even x
+// extent; 18-real FP32 links.  eta_mu for mu >= 1 is opposite on the two
+// lanes (x and x + 1).
+// ---------------------------------------------------------------------------
+LMB_D void su3_mul_vec2(const Cx2 *u, const Cx2 *v, Cx2 *o) {
+#pragma unroll
+  for (int r = 0; r < 3; r++) o[r] = cfma(u[r + 6], v[2], cfma(u[r + 3], v[1], u[r] * v[0]));
+}
+LMB_D void su3_adj_mul_vec2(const Cx2 *u, const Cx2 *v, Cx2 *o) {
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    const Cx2 a = u[3 * r], b = v[0];
+    const Cx2 t(fma2(a.im, b.im, a.re * b.re), fma2(-a.im, b.re, a.re * b.im));
+    o[r] = cfma_conj(u[3 * r + 2], v[2], cfma_conj(u[3 * r + 1], v[1], t));
+  }
+}
+LMB_D void phase_t_sel(const Geom &g, int wraps, Cx2 *v) {
+  const double *ph = wraps > 0 ? g.ph_fwd[3] : g.ph_bwd[3];
+  const float pr = wraps ? (float)ph[0] : 1.f, pi = wraps ? (float)ph[1] : 0.f;
+  const Cx2 f(f2(pr), f2(pi));
+#pragma unroll
+  for (int i = 0; i < 3; i++) v[i] = v[i] * f;
+}
+
+// acc += eta [U(x) psi(x + D mu) - U(x - D mu)^+ psi(x - D mu)]
+template <int MU, int D>
+LMB_D void stag_hop_adj(const Geom &g, int s0, const int *c0, const int *c1, const Field<PREC_SINGLE, 3> &in,
+                        const Gauge<PREC_SINGLE> &U, float2 eta, Cx2 *acc) {
+  Cx2 v[3], u[9], o[3];
+  int w0, w1;
+  if constexpr (MU == 0) {
+    const int n0 = shift_site_sel(g, s0, c0, 0, D, &w0), n1 = shift_site_sel(g, s0 + 1, c1, 0, D, &w1);
+    load2(in, n0, n1, v);
+  } else {
+    const int n = (D == 1) ? fwd_site(g, s0, c0, MU, 1, &w0) : shift_site_sel(g, s0, c0, MU, D, &w0);
+    load_adj(in, n, v);
+    if constexpr (MU == 3) phase_t_sel(g, w0, v);
+  }
+  load_adj(U, MU, s0, u);
+  su3_mul_vec2(u, v, o);
+#pragma unroll
+  for (int i = 0; i < 3; i++) acc[i] = Cx2(fma2(eta, o[i].re, acc[i].re), fma2(eta, o[i].im, acc[i].im));
+  if constexpr (MU == 0) {
+    const int n0 = shift_site_sel(g, s0, c0, 0, -D, &w0), n1 = shift_site_sel(g, s0 + 1, c1, 0, -D, &w1);
+    load2(in, n0, n1, v);
+    load2(U, 0, n0, n1, u);
+  } else {
+    const int n = (D == 1) ? bwd_site(g, s0, c0, MU, 1, &w0) : shift_site_sel(g, s0, c0, MU, -D, &w0);
+    if (D == 1 && w0) w0 = -1;
+    load_adj(in, n, v);
+    if constexpr (MU == 3) phase_t_sel(g, w0, v);
+    load_adj(U, MU, n, u);
+  }
+  su3_adj_mul_vec2(u, v, o);
+#pragma unroll
+  for (int i = 0; i < 3; i++) acc[i] = Cx2(fma2(-eta, o[i].re, acc[i].re), fma2(-eta, o[i].im, acc[i].im));
+}
+
+// V/2 threads.  Epi must provide skip() and pair_adj(s0, active, out[3]).
+template <bool NAIK, class Epi>
+__global__ void __launch_bounds__(kStagThreads, LMB_PAIR_MINB)
+    staggered_adj_kernel(const Geom g, const Field<PREC_SINGLE, 3> in, const Gauge<PREC_SINGLE> X,
+                         const Gauge<PREC_SINGLE> Lk, const float mass, const float fc, const float lc, Epi epi) {
+  if (epi.skip()) return;
+  const int i = blockIdx.x * kStagThreads + threadIdx.x;
+  const bool active = i < (int)(g.V >> 1);
+  const int s0 = 2 * i;
+  Cx2 out[3];
+  if (active) {
+    int c0[4], c1[4];
+    site_coords(g, s0, c0);
+    c1[0] = c0[0] + 1;
+    c1[1] = c0[1];
+    c1[2] = c0[2];
+    c1[3] = c0[3];
+    const int p0 = c0[0] + g.eta_off[0], p1 = p0 + c0[1] + g.eta_off[1], p2 = p1 + c0[2] + g.eta_off[2];
+    const float e1 = (p0 & 1) ? -1.f : 1.f, e2 = (p1 & 1) ? -1.f : 1.f, e3 = (p2 & 1) ? -1.f : 1.f;
+    const float2 eta0 = f2(1.f), eta1 = f2(e1, -e1), eta2 = f2(e2, -e2), eta3 = f2(e3, -e3);
+    Cx2 fat[3] = {cx2_zero(), cx2_zero(), cx2_zero()};
+    stag_hop_adj<0, 1>(g, s0, c0, c1, in, X, eta0, fat);
+    stag_hop_adj<1, 1>(g, s0, c0, c1, in, X, eta1, fat);
+    stag_hop_adj<2, 1>(g, s0, c0, c1, in, X, eta2, fat);
+    stag_hop_adj<3, 1>(g, s0, c0, c1, in, X, eta3, fat);
+    Cx2 psi[3];
+    load_adj(in, s0, psi);
+    const float2 m2 = f2(mass), f2c = f2(fc);
+    if constexpr (NAIK) {
+      Cx2 lng[3] = {cx2_zero(), cx2_zero(), cx2_zero()};
+      stag_hop_adj<0, 3>(g, s0, c0, c1, in, Lk, eta0, lng);
+      stag_hop_adj<1, 3>(g, s0, c0, c1, in, Lk, eta1, lng);
+      stag_hop_adj<2, 3>(g, s0, c0, c1, in, Lk, eta2, lng);
+      stag_hop_adj<3, 3>(g, s0, c0, c1, in, Lk, eta3, lng);
+      const float2 l2 = f2(lc);
+#pragma unroll
+      for (int k = 0; k < 3; k++)
+        out[k] = Cx2(fma2(l2, lng[k].re, fma2(f2c, fat[k].re, m2 * psi[k].re)),
+                     fma2(l2, lng[k].im, fma2(f2c, fat[k].im, m2 * psi[k].im)));
+    } else {
+#pragma unroll
+      for (int k = 0; k < 3; k++)
+        out[k] = Cx2(fma2(f2c, fat[k].re, m2 * psi[k].re), fma2(f2c, fat[k].im, m2 * psi[k].im));
+    }
+  }
+  epi.pair_adj(s0, active, out);
+}
+
 }  // namespace lmb
