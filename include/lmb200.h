@@ -193,6 +193,31 @@ int lmb_hisq_fermion_force(lmb_ctx *ctx, const void *const U[4],
                            void *const dU[4], const lmb_cg_params *cg,
                            lmb_cg_result *result, void *stream);
 
+/* wilson_clover_link_pullback!(dU, cache, U, result_cotangent, psi;
+ * coefficient) (Operators/WilsonCloverPullback.jl:342-403): accumulates into
+ * the four padded link fields dU the gradient G of f = coefficient
+ * Re<result_cotangent, D(U) psi> for the Wilson-clover operator with kappa,
+ * cSW (df = Re sum conj(G) dU): hopping outer products and, through
+ * F_mu_nu = (Q - Q^+)/8, the four-leaf clover term.  FP64.  dU must not alias
+ * U; the fields share the context geometry. */
+int lmb_wilson_clover_link_pullback(lmb_ctx *ctx, const void *const U[4],
+                                    double kappa, double csw,
+                                    double coefficient,
+                                    const void *result_cotangent,
+                                    const void *psi, void *const dU[4],
+                                    void *stream);
+
+/* Fermion force dS/dU of S = phi^+ (D^+D)^-1 phi for the Wilson-clover
+ * operator (the clover counterpart of lmb_hisq_fermion_force; dSFdU,
+ * ext/LatticeMatricesEnzymeExt.jl:387-460): uploads U (epoch = halo_epoch.core),
+ * solves eta = (D^+D)^-1 phi with lmb_cg_ddagd (cg->precision, rtol, ...),
+ * chi = D eta, then accumulates -2 d/dU Re<chi, D(U) eta> into dU. */
+int lmb_wilson_clover_fermion_force(lmb_ctx *ctx, const void *const U[4],
+                                    const uint64_t epoch[4], double kappa,
+                                    double csw, const void *phi,
+                                    void *const dU[4], const lmb_cg_params *cg,
+                                    lmb_cg_result *result, void *stream);
+
 /* CloverFieldStrength4D(U) components (12,13,14,23,24,34) written to six
  * padded (3,3,...) fields (Operators/WilsonDiracCloverOperator.jl:28-35,
  * 392-399). */

@@ -11,6 +11,7 @@
 #include "lmb_hisq_smear.cuh"
 #include "lmb_batch.cuh"
 #include "lmb_hisq_force.cuh"
+#include "lmb_clover_force.cuh"
 
 using namespace lmb;
 
@@ -1350,6 +1351,27 @@ int hisq_pullback_planes(lmb_ctx *ctx, const double2 *thin, const Field<PREC_DOU
   return fat7_pullback_planes(ctx, thin, dV1, dU, c_level1, st);
 }
 
+// grad (36 planes) += d/dU [coef Re<dr, D_clover(U) psi>]
+int clover_pullback_planes(lmb_ctx *ctx, const double2 *thin, const Field<PREC_DOUBLE, 12> &dr,
+                           const Field<PREC_DOUBLE, 12> &psi, double kappa, double csw, double coefficient,
+                           double2 *grad, cudaStream_t st) {
+  const int64_t n = ctx->g.V;
+  wilson_outer_product_kernel<<<grid_for(n, 128), 128, 0, st>>>(grad, dr, psi, ctx->g, -kappa * coefficient);
+  LMB_CHECK_LAUNCH(ctx);
+  if (csw == 0.0) return LMB_OK;
+  double2 *dF = (double2 *)workspace(ctx, "force_dF", sizeof(double2) * 54 * n);
+  if (!dF) return fail(ctx, LMB_ERR_CUDA, "out of device memory (clover force)");
+  clover_cotangent_kernel<<<grid_for(n, 128), 128, 0, st>>>(dF, dr, psi, ctx->g, -kappa * csw * coefficient);
+  LMB_CHECK_LAUNCH(ctx);
+  static const int pmu[6] = {0, 0, 0, 1, 1, 2}, pnu[6] = {1, 2, 3, 2, 3, 3};
+  for (int plane = 0; plane < 6; plane++) {
+    clover_link_pullback_kernel<<<grid_for(n, 64), 64, 0, st>>>(grad, thin, dF, ctx->g, plane, pmu[plane],
+                                                                 pnu[plane]);
+    LMB_CHECK_LAUNCH(ctx);
+  }
+  return LMB_OK;
+}
+
 int accumulate_links_to(lmb_ctx *ctx, void *const dU[4], const double2 *planes, cudaStream_t st) {
   const unsigned grid = grid_for(ctx->g.V, 256);
   if (ctx->dtype == LMB_DTYPE_C128)
@@ -1814,6 +1836,64 @@ int lmb_hisq_fermion_force(lmb_ctx *ctx, const void *const U[4], const uint64_t 
   // dS/dU = -2 d/dU Re<chi, D(U) eta> with chi, eta fixed (dSFdU,
   // ext/LatticeMatricesEnzymeExt.jl:387-460)
   return lmb_hisq_link_pullback(ctx, U, naik_epsilon, -2.0, chi, eta, dU, stream);
+}
+
+int lmb_wilson_clover_link_pullback(lmb_ctx *ctx, const void *const U[4], double kappa, double csw,
+                                    double coefficient, const void *result_cotangent, const void *psi,
+                                    void *const dU[4], void *stream) {
+  if (!ctx_ok(ctx)) return LMB_ERR_ARG;
+  if (!ctx->geom_set) return fail(ctx, LMB_ERR_STATE, "lmb_set_geometry has not been called");
+  int rc = check_links_arg(ctx, U, "primal link");
+  if (rc) return rc;
+  if ((rc = check_links_arg(ctx, (const void *const *)dU, "link cotangent"))) return rc;
+  if (!result_cotangent || !psi) return fail(ctx, LMB_ERR_ARG, "null fermion field");
+  if (!std::isfinite(kappa) || !std::isfinite(csw) || !std::isfinite(coefficient))
+    return fail(ctx, LMB_ERR_ARG, "kappa, cSW and coefficient must be finite");
+  for (int mu = 0; mu < 4; mu++)
+    for (int nu = 0; nu < 4; nu++)
+      if (dU[mu] == U[nu])
+        return fail(ctx, LMB_ERR_ARG, "Wilson--clover link cotangents must not alias primal links");
+  cudaStream_t st = as_stream(stream);
+  const int64_t n = ctx->g.V;
+  double2 *thin = (double2 *)workspace(ctx, "force_thin", sizeof(double2) * 36 * n);
+  double2 *grad = (double2 *)workspace(ctx, "force_grad", sizeof(double2) * 36 * n);
+  Field<PREC_DOUBLE, 12> dr, ps;
+  if (!thin || !grad || !make_field(ctx, "force_dr12", dr) || !make_field(ctx, "force_psi12", ps))
+    return fail(ctx, LMB_ERR_CUDA, "out of device memory (force)");
+  if ((rc = pack_links_to(ctx, thin, U, st))) return rc;
+  if ((rc = pack_in(ctx, dr, result_cotangent, st))) return rc;
+  if ((rc = pack_in(ctx, ps, psi, st))) return rc;
+  LMB_CUDA(ctx, cudaMemsetAsync(grad, 0, sizeof(double2) * 36 * n, st));
+  if ((rc = clover_pullback_planes(ctx, thin, dr, ps, kappa, csw, coefficient, grad, st))) return rc;
+  return accumulate_links_to(ctx, dU, grad, st);
+}
+
+int lmb_wilson_clover_fermion_force(lmb_ctx *ctx, const void *const U[4], const uint64_t epoch[4], double kappa,
+                                    double csw, const void *phi, void *const dU[4], const lmb_cg_params *cg,
+                                    lmb_cg_result *result, void *stream) {
+  if (!ctx_ok(ctx)) return LMB_ERR_ARG;
+  if (!ctx->geom_set) return fail(ctx, LMB_ERR_STATE, "lmb_set_geometry has not been called");
+  if (!cg || !result || !phi || !epoch) return fail(ctx, LMB_ERR_ARG, "null argument");
+  int rc = check_links_arg(ctx, U, "primal link");
+  if (rc) return rc;
+  if ((rc = check_links_arg(ctx, (const void *const *)dU, "force"))) return rc;
+  cudaStream_t st = as_stream(stream);
+  if ((rc = lmb_links_upload(ctx, LMB_LINKS_THIN, U, epoch, stream))) return rc;
+  // eta = (D^+D)^-1 phi, chi = D eta, in padded scratch fields of the context geometry
+  size_t padded = 12;
+  for (int mu = 0; mu < 4; mu++) padded *= (size_t)ctx->pd.P[mu];
+  const size_t elem = ctx->dtype == LMB_DTYPE_C128 ? 16 : 8;
+  void *eta = workspace(ctx, "force_eta12", padded * elem), *chi = workspace(ctx, "force_chi12", padded * elem);
+  if (!eta || !chi) return fail(ctx, LMB_ERR_CUDA, "out of device memory (force fields)");
+  LMB_CUDA(ctx, cudaMemsetAsync(eta, 0, padded * elem, st));
+  lmb_cg_params prm = *cg;
+  prm.op = csw != 0.0 ? LMB_OP_WILSON_CLOVER : LMB_OP_WILSON;
+  prm.kappa = kappa;
+  prm.csw = csw;
+  if ((rc = lmb_cg_ddagd(ctx, &prm, eta, phi, result, stream))) return rc;
+  if ((rc = apply_dispatch(ctx, WilsonPolicy{prm.op, kappa, csw}, chi, eta, 0, PREC_DOUBLE, stream))) return rc;
+  // dS/dU = -2 d/dU Re<chi, D(U) eta> with chi, eta fixed
+  return lmb_wilson_clover_link_pullback(ctx, U, kappa, csw, -2.0, chi, eta, dU, stream);
 }
 
 }  // extern "C"

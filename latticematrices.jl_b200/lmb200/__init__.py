@@ -19,6 +19,7 @@ from .hisq import (HISQDiracCache4D, hisq_fat7_level1_,  # noqa: F401
                    hisq_fat7_level2_, hisq_links_from_thin, hisq_naik_links_,
                    hisq_project_u3_, mul_cached_hisq_,
                    mul_cached_hisq_adjoint_)
+from .clover import wilson_clover_fermion_force_, wilson_clover_link_pullback_  # noqa: F401
 from .inputs import gaussian_fermion, random_su3_links  # noqa: F401
 from .solver import (CGResult, DdagDOp, cg_, cg_batched_, dot,  # noqa: F401
                      pseudofermion_action, solve_)

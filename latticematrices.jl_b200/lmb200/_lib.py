@@ -37,6 +37,7 @@ EXPORTED = (
     "lmb_hisq_fat7", "lmb_hisq_project_u3", "lmb_hisq_naik",
     "lmb_hisq_links_from_thin", "lmb_cg_ddagd_batched",
     "lmb_hisq_link_pullback", "lmb_hisq_fermion_force",
+    "lmb_wilson_clover_link_pullback", "lmb_wilson_clover_fermion_force",
 )
 
 
@@ -143,6 +144,13 @@ def load(path: str = LIB_PATH):
             vp, ctypes.POINTER(vp), ctypes.c_double, ctypes.c_double, vp, vp,
             ctypes.POINTER(vp), vp]
         lib.lmb_hisq_fermion_force.argtypes = [
+            vp, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_uint64),
+            ctypes.c_double, ctypes.c_double, vp, ctypes.POINTER(vp),
+            ctypes.POINTER(CGParams), ctypes.POINTER(CGResultC), vp]
+        lib.lmb_wilson_clover_link_pullback.argtypes = [
+            vp, ctypes.POINTER(vp), ctypes.c_double, ctypes.c_double,
+            ctypes.c_double, vp, vp, ctypes.POINTER(vp), vp]
+        lib.lmb_wilson_clover_fermion_force.argtypes = [
             vp, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_uint64),
             ctypes.c_double, ctypes.c_double, vp, ctypes.POINTER(vp),
             ctypes.POINTER(CGParams), ctypes.POINTER(CGResultC), vp]
