@@ -94,12 +94,13 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
     ap.add_argument("--workload", default="clover",
-                    choices=["clover", "wilson8", "hisq", "batched", "force"],
+                    choices=["clover", "wilson8", "hisq", "batched", "force", "clover_force"],
                     help="clover: 32^3x64 Wilson-clover mixed vs FP64 CG (the "
                          "headline line); wilson8: 8^4 Wilson FP64 CG beside the "
                          "CPU oracle; hisq: 48^3x96 HISQ smearing + CG; batched: "
                          "multi-RHS multi-lattice Wilson CG; force: 24^4 HISQ "
-                         "fermion force with a finite-difference check")
+                         "fermion force with a finite-difference check; "
+                         "clover_force: 24^4 Wilson-clover fermion force, same check")
     ap.add_argument("--fd-directions", type=int, default=64)
     return ap.parse_args()
 
@@ -676,6 +677,63 @@ def run_force(args):
           flush=True)
 
 
+def run_clover_force(args):
+    """Wilson-clover fermion force dS/dU, S = phi^+ (D^+D)^-1 phi, on 24^4
+    (kappa 0.1355, cSW 1.0, links exp(0.2 i H)), checked by central finite
+    differences (eps 1e-5) along random link directions with the
+    difference-solve form of run_force."""
+    import numpy as np
+    import torch
+    import lmb200 as lmb
+    L = tuple(int(v) for v in (args.lattice if args.lattice != "32,32,32,64"
+                                else "24,24,24,24").split(","))
+    kappa, csw = args.kappa, args.csw
+    U = lmb.random_su3_links(L, 0.2, 1)
+    phi = lmb.gaussian_fermion(L, 3, 4, 2, phases=PHASES)
+    D = lmb.WilsonDiracCloverOperator4D(U, kappa, csw)
+    dU = [u.similar() for u in U]
+    st = torch.cuda.current_stream()
+    lmb.wilson_clover_fermion_force_(dU, D, phi, rtol=1e-12)
+    for d in dU:
+        lmb.clear_matrix_(d)
+    res, t_force = _timed(lambda: lmb.wilson_clover_fermion_force_(dU, D, phi, rtol=1e-12), st)
+    G = [d.core_view().clone() for d in dU]
+    base = [u.core_view().clone() for u in U]
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    h = 1e-5
+    x0, t, r, d = phi.similar(), phi.similar(), phi.similar(), phi.similar()
+    lmb.cg_(x0, lmb.DdagDOp(D, phi.similar()), phi, rtol=1e-12, maxiter=50000)
+
+    def side(sign, V):
+        for u, b, v in zip(U, base, V):
+            u.core_view().copy_(b + sign * h * v)
+            lmb.mark_halo_dirty_(u)
+        A = lmb.DdagDOp(lmb.WilsonDiracCloverOperator4D(U, kappa, csw), phi.similar())
+        A.mul_(t, x0)
+        r.core_view().copy_(phi.core_view() - t.core_view())
+        lmb.mark_halo_dirty_(r)
+        lmb.clear_matrix_(d)
+        lmb.cg_(d, A, r, rtol=1e-12, maxiter=50000)
+        return lmb.dot(phi, d).real
+
+    ans, fds = [], []
+    for k in range(args.fd_directions):
+        V = [torch.randn(b.shape, dtype=b.dtype, device=b.device, generator=gen) for b in base]
+        fds.append((side(+1, V) - side(-1, V)) / (2 * h))
+        ans.append(sum(float((g.conj() * v).sum().real) for g, v in zip(G, V)))
+    for u, b in zip(U, base):
+        u.core_view().copy_(b)
+        lmb.mark_halo_dirty_(u)
+    ans, fds = np.array(ans), np.array(fds)
+    print(json.dumps({"workload": "Wilson-clover fermion force %dx%dx%dx%d kappa %g cSW %g" % (L + (kappa, csw)),
+                      "force_s": t_force, "cg_iterations": res.iterations,
+                      "fd_directions": args.fd_directions, "fd_eps": h,
+                      "max_rel_diff_vs_fd": float(np.max(np.abs(ans - fds) / np.abs(fds))),
+                      "max_diff_over_rms_fd": float(np.max(np.abs(ans - fds)) / np.sqrt(np.mean(fds ** 2))),
+                      "rel_diff_norm_vs_fd": float(np.linalg.norm(ans - fds) / np.linalg.norm(fds))}),
+          flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -686,7 +744,7 @@ def main():
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         {"wilson8": run_wilson8, "hisq": run_hisq, "batched": run_batched,
-         "force": run_force}[args.workload](args)
+         "force": run_force, "clover_force": run_clover_force}[args.workload](args)
 
 
 if __name__ == "__main__":
