@@ -170,6 +170,87 @@ void orc_wilson_donly(const int *L, const double *phases, int nc, int dagger,
 }
 
 /* ---------------------------------------------------------------------------
+ * Generalised domain-wall operator (DiracOperators_5D.jl:48-115, 226-268,
+ * 731-857; Mobius = a 1, b (b+c)/2, c (b-c)/2):
+ *   D5 psi = A [psi - F psi + D_W (B psi + C F psi)],
+ *   D5^+ psi = q - F^+ q + B D_W^+ q + F^+ (C D_W^+ q),  q = A psi,
+ * with A, B, C diagonal in the fifth coordinate s, the 4D Wilson kernel
+ *   D_W psi = (4 + M) psi - 1/2 sum_mu [U(1 - g)psi(x+mu) + U^+(1 + g)psi(x-mu)]
+ * on every s-slice (fermion phases in x..t), and
+ *   (F psi)_s   : spins 1,2 from s-1 (x (-mass) at s = 1), spins 3,4 from s+1
+ *                 (x (-mass) at s = L5);
+ *   (F^+ psi)_s : spins 1,2 from s+1 (x (-mass) at s = L5), spins 3,4 from s-1
+ *                 (x (-mass) at s = 1).
+ * Fields: (nc, 4, X, Y, Z, T, L5) column-major, slices contiguous.
+ * ------------------------------------------------------------------------- */
+static void dw_F(const int *L, int L5, int nc, double mass, int adj, const cplx *in, cplx *out) {
+  const int64_t V4 = volume_of(L), n4 = (int64_t)nc * 4 * V4;
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n4 * L5; i++) {
+    const int s = (int)(i / n4);
+    const int64_t r = i - (int64_t)s * n4;
+    const int spin = (int)((r / nc) % 4);
+    const int low = spin < 2;
+    int src;
+    double coef = 1.0;
+    if (!adj) {
+      src = low ? (s + L5 - 1) % L5 : (s + 1) % L5;
+      if (low && s == 0) coef = -mass;
+      if (!low && s == L5 - 1) coef = -mass;
+    } else {
+      src = low ? (s + 1) % L5 : (s + L5 - 1) % L5;
+      if (low && s == L5 - 1) coef = -mass;
+      if (!low && s == 0) coef = -mass;
+    }
+    out[i] = coef * in[r + (int64_t)src * n4];
+  }
+}
+
+static void dw_wilson(const int *L, int L5, const double *phases, int nc, double M, int dagger,
+                      const double *const *U, const cplx *in, cplx *out) {
+  const int64_t n4 = (int64_t)nc * 4 * volume_of(L);
+  for (int s = 0; s < L5; s++) {
+    wilson_generic(L, phases, nc, -0.5, 0, dagger, U, (const double *)(in + s * n4),
+                   (double *)(out + s * n4));
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n4; i++) out[s * n4 + i] += (4.0 + M) * in[s * n4 + i];
+  }
+}
+
+void orc_domainwall(const int *L, int L5, const double *phases, int nc, double mass, double M,
+                    const double *a, const double *b, const double *c, int dagger,
+                    const double *const *U, const double *psid, double *outd) {
+  const int64_t n4 = (int64_t)nc * 4 * volume_of(L), n = n4 * L5;
+  const cplx *psi = (const cplx *)psid;
+  cplx *out = (cplx *)outd;
+  cplx *t1 = (cplx *)malloc(sizeof(cplx) * n), *t2 = (cplx *)malloc(sizeof(cplx) * n);
+  cplx *t3 = (cplx *)malloc(sizeof(cplx) * n);
+  if (!dagger) {
+    dw_F(L, L5, nc, mass, 0, psi, t1);  /* F psi */
+    for (int64_t i = 0; i < n; i++) {
+      const int s = (int)(i / n4);
+      t2[i] = b[s] * psi[i] + c[s] * t1[i];  /* B psi + C F psi */
+    }
+    dw_wilson(L, L5, phases, nc, M, 0, U, t2, t3);
+    for (int64_t i = 0; i < n; i++) {
+      const int s = (int)(i / n4);
+      out[i] = a[s] * (psi[i] - t1[i] + t3[i]);
+    }
+  } else {
+    for (int64_t i = 0; i < n; i++) t1[i] = a[i / n4] * psi[i];  /* q */
+    dw_wilson(L, L5, phases, nc, M, 1, U, t1, t2);                /* D_W^+ q */
+    dw_F(L, L5, nc, mass, 1, t1, t3);                             /* F^+ q */
+    for (int64_t i = 0; i < n; i++) out[i] = t1[i] - t3[i] + b[i / n4] * t2[i];
+    for (int64_t i = 0; i < n; i++) t2[i] = c[i / n4] * t2[i];    /* C D_W^+ q */
+    dw_F(L, L5, nc, mass, 1, t2, t3);
+    for (int64_t i = 0; i < n; i++) out[i] += t3[i];
+  }
+  free(t1);
+  free(t2);
+  free(t3);
+}
+
+/* ---------------------------------------------------------------------------
  * small dense matrix helpers (column-major NC x NC, as the reference stores
  * U[row, col, site])
  * ------------------------------------------------------------------------- */

@@ -26,6 +26,11 @@ extern "C" {
 /* geometry: L[4] lattice extents, phases[8] = (re, im) per direction,
  * eta_offset[4] = global coordinate of the local origin (0 on one rank). */
 
+/* generalised domain-wall operator D5 (dagger = 1: D5^+), fields
+ * (nc, 4, X, Y, Z, T, L5); a, b, c: L5 coefficients each */
+void orc_domainwall(const int *L, int L5, const double *phases, int nc, double mass, double M,
+                    const double *a, const double *b, const double *c, int dagger,
+                    const double *const *U, const double *psi, double *out);
 void orc_wilson(const int *L, const double *phases, int nc, double kappa,
                 int dagger, const double *const *U, const double *psi,
                 double *out);

@@ -158,6 +158,26 @@ def staggered(U, psi, mass, phases=(1, 1, 1, -1), dagger=False,
     return out
 
 
+def domainwall(U, psi, mass, M, a, b, c, phases=(1, 1, 1, -1), dagger=False):
+    """Generalised domain-wall D5 (or D5^+) on a (nc, 4, X, Y, Z, T, L5)
+    field; a, b, c: L5 coefficients (Mobius: ones, (b+c)/2, (b-c)/2)."""
+    L = tuple(int(v) for v in psi.shape[2:6])
+    L5 = int(psi.shape[6])
+    dvec = lambda v: (ctypes.c_double * L5)(*[float(x) for x in v])
+    out = np.zeros(psi.shape, dtype=np.complex128, order="F")
+    lib().orc_domainwall(_ivec(L), L5, _phases(phases), psi.shape[0],
+                         ctypes.c_double(mass), ctypes.c_double(M), dvec(a),
+                         dvec(b), dvec(c), int(dagger),
+                         _ptrs([_check(u) for u in U]), _ptr(_check(psi)),
+                         _ptr(out))
+    return out
+
+
+def mobius_coefficients(L5, b, c):
+    """D5DW_MobiusDomainwallOperator5D(b, c) as the generalised operator."""
+    return [1.0] * L5, [(b + c) / 2] * L5, [(b - c) / 2] * L5
+
+
 def hisq(X, Lng, psi, mass, naik_epsilon=0.0, phases=(1, 1, 1, -1),
          dagger=False, eta_offset=(0, 0, 0, 0)):
     L = lattice_shape(psi)

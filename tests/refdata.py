@@ -388,3 +388,72 @@ def plane_wave(L, momentum):
 def rel_err(a, b):
     return float(np.linalg.norm((a - b).ravel()) /
                  max(np.linalg.norm(np.asarray(b).ravel()), 1e-300))
+
+
+# ---------------------------------------------------------------------------
+# domain wall (test/domainwall.jl:1-127): recipe and dense oracle
+# ---------------------------------------------------------------------------
+def domainwall_test_values(n1, n2, size, offset):
+    """test/domainwall.jl:20-32 over a lattice of any rank (1-based coords)."""
+    out = np.zeros((n1, n2) + tuple(size), dtype=np.complex128, order="F")
+    for pos in itertools.product(*[range(1, n + 1) for n in size]):
+        coordinate = sum((2 * (d + 1) - 1) * pos[d] for d in range(len(size)))
+        for second in range(1, n2 + 1):
+            for first in range(1, n1 + 1):
+                out[(first - 1, second - 1) + tuple(p - 1 for p in pos)] = (
+                    0.013 * (first + 2 * second + coordinate + offset) +
+                    1j * 0.017 * (2 * first - second - coordinate + offset))
+    return out
+
+
+def domainwall_F_dense(psi, mass, adjoint=False):
+    """test/domainwall.jl:34-55."""
+    L5 = psi.shape[6]
+    out = np.empty_like(psi)
+    for s in range(1, L5 + 1):
+        if adjoint:
+            lo, hi = (s % L5) + 1, ((s - 2) % L5) + 1
+            clo = -mass if s == L5 else 1.0
+            chi = -mass if s == 1 else 1.0
+        else:
+            lo, hi = ((s - 2) % L5) + 1, (s % L5) + 1
+            clo = -mass if s == 1 else 1.0
+            chi = -mass if s == L5 else 1.0
+        out[:, 0:2, ..., s - 1] = clo * psi[:, 0:2, ..., lo - 1]
+        out[:, 2:4, ..., s - 1] = chi * psi[:, 2:4, ..., hi - 1]
+    return out
+
+
+def domainwall_DW_dense(links, psi, M, phases, adjoint=False):
+    """test/domainwall.jl:57-86: (4+M) psi - 1/2 sum_mu hops on every slice."""
+    L = psi.shape[2:6]
+    L5 = psi.shape[6]
+    out = np.empty_like(psi)
+    eye = np.eye(4, dtype=complex)
+    for s in range(L5):
+        for x in sites(L):
+            value = (4 + M) * psi[(slice(None), slice(None)) + idx(x) + (s,)].copy()
+            for mu in range(4):
+                xp, php = fermion_shift(x, mu, 1, L, phases)
+                xm, phm = fermion_shift(x, mu, -1, L, phases)
+                gf = eye + GAMMA[mu] if adjoint else eye - GAMMA[mu]
+                gb = eye - GAMMA[mu] if adjoint else eye + GAMMA[mu]
+                value -= 0.5 * mat(links[mu], x) @ (php * psi[(slice(None), slice(None)) + idx(xp) + (s,)]) @ gf.T
+                value -= 0.5 * mat(links[mu], xm).conj().T @ (
+                    phm * psi[(slice(None), slice(None)) + idx(xm) + (s,)]) @ gb.T
+            out[(slice(None), slice(None)) + idx(x) + (s,)] = value
+    return out
+
+
+def domainwall_dense(links, psi, mass, M, a, b, c, phases, adjoint=False):
+    """test/domainwall.jl:107-127 (generalised operator and its adjoint)."""
+    A = np.asarray(a).reshape((1,) * 6 + (-1,))
+    B = np.asarray(b).reshape((1,) * 6 + (-1,))
+    C = np.asarray(c).reshape((1,) * 6 + (-1,))
+    if adjoint:
+        q = A * psi
+        Fq = domainwall_F_dense(q, mass, adjoint=True)
+        Dq = domainwall_DW_dense(links, q, M, phases, adjoint=True)
+        return q - Fq + B * Dq + domainwall_F_dense(C * Dq, mass, adjoint=True)
+    Fpsi = domainwall_F_dense(psi, mass)
+    return A * (psi - Fpsi + domainwall_DW_dense(links, B * psi + C * Fpsi, M, phases))

@@ -310,3 +310,28 @@ def test_philox_known_answer(orc):
         0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8)
     assert orc.philox4x32((0xffffffff,) * 4, (0xffffffff,) * 2) == (
         0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd)
+
+
+DW_PHASES = (np.exp(0.13j), np.exp(-0.21j), np.exp(0.34j), np.exp(1j * (np.pi - 0.17)))
+
+
+@pytest.mark.parametrize("nc", [2, 3])
+def test_domainwall_matches_reference_dense_oracle(orc, nc):
+    """test/domainwall.jl:205-299: Mobius (b, c) in {(1,1), (2,0), (2,1)} and a
+    generalised operator on the reference's deterministic inputs (lattice
+    2^4, L5 = 3, mass 0.13, M = -1, twisted phases), at its 8e-12 bars."""
+    L, L5, mass, M = (2, 2, 2, 2), 3, 0.13, -1.0
+    links = [np.asfortranarray(rd.domainwall_test_values(nc, nc, L, 7 * (mu + 1))) for mu in range(4)]
+    psi = np.asfortranarray(rd.domainwall_test_values(nc, 4, L + (L5,), 11))
+    left = np.asfortranarray(rd.domainwall_test_values(nc, 4, L + (L5,), 23))
+    cases = [orc.mobius_coefficients(L5, b, c) for b, c in ((1.0, 1.0), (2.0, 0.0), (2.0, 1.0))]
+    cases.append(([0.83, 1.17, 1.31], [1.2, 0.91, 1.47], [-0.18, 0.37, 0.22]))
+    for a, b, c in cases:
+        got = orc.domainwall(links, psi, mass, M, a, b, c, DW_PHASES)
+        ref = rd.domainwall_dense(links, psi, mass, M, a, b, c, DW_PHASES)
+        assert np.allclose(got, ref, atol=8e-12, rtol=8e-12)
+        gotd = orc.domainwall(links, left, mass, M, a, b, c, DW_PHASES, dagger=True)
+        refd = rd.domainwall_dense(links, left, mass, M, a, b, c, DW_PHASES, adjoint=True)
+        assert np.allclose(gotd, refd, atol=8e-12, rtol=8e-12)
+        # <left, D psi> = <D^+ left, psi>
+        assert np.isclose(np.vdot(left, got), np.vdot(gotd, psi), atol=2e-10, rtol=2e-11)
