@@ -42,6 +42,7 @@ extern "C" {
 #define LMB_OP_WILSON_CLOVER 1
 #define LMB_OP_STAGGERED 2
 #define LMB_OP_HISQ 3
+#define LMB_OP_DOMAINWALL 4 /* lmb_domainwall_set parameters, 5D fields */
 
 #define LMB_LINKS_THIN 0 /* Wilson / clover / staggered links U_mu      */
 #define LMB_LINKS_FAT 1  /* HISQ fat links X_mu (HISQLinks4D)           */
@@ -192,6 +193,25 @@ int lmb_hisq_fermion_force(lmb_ctx *ctx, const void *const U[4],
                            double naik_epsilon, const void *phi,
                            void *const dU[4], const lmb_cg_params *cg,
                            lmb_cg_result *result, void *stream);
+
+/* D5DW_GeneralizedDomainwallOperator5D(U, L5, mass, M, a, b, c)
+ * (Operators/DiracOperators_5D.jl:48-115, 204-268; Mobius(b, c) is a = 1,
+ * b_s = (b + c)/2, c_s = (b - c)/2, :8-46, 171-202):
+ *   D5 psi = A [psi - F psi + D_W (B psi + C F psi)],
+ * D_W the 4D Wilson kernel (4 + M) - 1/2 hopping with the uploaded links
+ * (LMB_LINKS_THIN) and the geometry's phases, F the chiral fifth-coordinate
+ * hop with -mass across the walls.  Sets the parameters used by
+ * lmb_domainwall_apply and by lmb_cg_ddagd with op = LMB_OP_DOMAINWALL; a, b,
+ * c hold L5 values each (copied).  Synchronises the stream. */
+int lmb_domainwall_set(lmb_ctx *ctx, int L5, double mass, double M,
+                       const double *a, const double *b, const double *c,
+                       void *stream);
+
+/* mul!(out, D5DW_*DomainwallOperator5D, in) / adjoint (DiracOperators_5D.jl:
+ * 171-268, 1500-2084) on 5D padded fields (NC=3, 4, X+2nw, .., T+2nw,
+ * L5+2nw) of the context geometry. */
+int lmb_domainwall_apply(lmb_ctx *ctx, void *out, const void *in, int dagger,
+                         int precision, void *stream);
 
 /* wilson_clover_link_pullback!(dU, cache, U, result_cotangent, psi;
  * coefficient) (Operators/WilsonCloverPullback.jl:342-403): accumulates into

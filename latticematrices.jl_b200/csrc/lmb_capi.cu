@@ -12,6 +12,7 @@
 #include "lmb_batch.cuh"
 #include "lmb_hisq_force.cuh"
 #include "lmb_clover_force.cuh"
+#include "lmb_domainwall.cuh"
 
 using namespace lmb;
 
@@ -344,6 +345,51 @@ struct StaggeredPolicy {
   }
 };
 
+// generalised / Mobius domain-wall operator on V4 * L5 sites
+// (lmb_domainwall_set gives L5, mass, M, a, b, c)
+struct DWPolicy {
+  static constexpr int NC = 12;
+  int prepare(lmb_ctx *ctx, int prec, cudaStream_t st) const {
+    if (!ctx->geom_set) return fail(ctx, LMB_ERR_STATE, "lmb_set_geometry has not been called");
+    if (!ctx->links[LMB_LINKS_THIN].valid) return fail(ctx, LMB_ERR_STATE, "gauge links have not been uploaded");
+    if (ctx->dw_L5 <= 0) return fail(ctx, LMB_ERR_STATE, "lmb_domainwall_set has not been called");
+    int rc = check_prec(ctx, prec);
+    if (rc) return rc;
+    return ensure_link_precision(ctx, ctx->links[LMB_LINKS_THIN], prec, st);
+  }
+  DWParams params(const lmb_ctx *ctx) const {
+    const int L5 = ctx->dw_L5;
+    return DWParams{L5, ctx->dw_mass, ctx->dw_M, ctx->dw_coef, ctx->dw_coef + L5, ctx->dw_coef + 2 * L5};
+  }
+  template <int P, class G, class Epi>
+  int launch_g(lmb_ctx *ctx, const Field<P, 12> &in, const G &U, int dagger, const Epi &epi, cudaStream_t st) const {
+    typedef typename Real<P>::type R;
+    const int64_t V4 = ctx->g.V, V5 = V4 * ctx->dw_L5;
+    Field<P, 12> tmp;
+    if (!make_field(ctx, P == PREC_DOUBLE ? "dw_tmp_d" : (P == PREC_SINGLE ? "dw_tmp_s" : "dw_tmp_h"), tmp, V5))
+      return fail(ctx, LMB_ERR_CUDA, "out of device memory (domain-wall workspace)");
+    const DWParams d = params(ctx);
+    const unsigned grid = grid_for(V5, kDslashThreads);
+    if (!dagger) {
+      dw_fifth_kernel<P><<<grid, kDslashThreads, 0, st>>>(tmp, in, V4, d, epi);
+      dw_stencil_kernel<R, 0, 1><<<grid, kDslashThreads, 0, st>>>(ctx->g, tmp, in, U, d, epi);
+    } else {
+      const EpiStoreFollow<P, Epi> e1{tmp, epi};
+      dw_stencil_kernel<R, 1, 0><<<grid, kDslashThreads, 0, st>>>(ctx->g, in, in, U, d, e1);
+      dw_adjoint_local_kernel<R><<<grid, kDslashThreads, 0, st>>>(in, tmp, V4, d, epi);
+    }
+    LMB_CHECK_LAUNCH(ctx);
+    return LMB_OK;
+  }
+  template <int P, class Epi>
+  int launch(lmb_ctx *ctx, const Field<P, 12> &in, int dagger, const Epi &epi, cudaStream_t st) const {
+    const LinkSet &ls = ctx->links[LMB_LINKS_THIN];
+    if (ls.recon(P)) return launch_g<P>(ctx, in, gauge12_view<P>(ls, ctx->g.V), dagger, epi, st);
+    return launch_g<P>(ctx, in, gauge_view<P>(ls, ctx->g.V), dagger, epi, st);
+  }
+  int link_reals(const lmb_ctx *ctx, int prec) const { return ctx->links[LMB_LINKS_THIN].recon(prec) ? 12 : 18; }
+};
+
 template <int PS, int NC>
 int pack_in(lmb_ctx *ctx, Field<PS, NC> &f, const void *src, cudaStream_t st) {
   const unsigned grid = grid_for(ctx->g.V, 256);
@@ -366,18 +412,52 @@ int unpack_out(lmb_ctx *ctx, void *dst, const Field<PS, NC> &f, cudaStream_t st)
   return LMB_OK;
 }
 
+// operator hooks with the 4D defaults: field volume, pack, unpack
+template <class Op> int64_t op_volume(const lmb_ctx *ctx, const Op &) { return ctx->g.V; }
+template <class Op, int PS, int NC>
+int op_pack_in(lmb_ctx *ctx, const Op &, Field<PS, NC> &f, const void *src, cudaStream_t st) {
+  return pack_in(ctx, f, src, st);
+}
+template <class Op, int PS, int NC>
+int op_unpack_out(lmb_ctx *ctx, const Op &, void *dst, const Field<PS, NC> &f, cudaStream_t st) {
+  return unpack_out(ctx, dst, f, st);
+}
+
+inline int64_t op_volume(const lmb_ctx *ctx, const DWPolicy &) { return ctx->g.V * ctx->dw_L5; }
+template <int PS, int NC>
+int op_pack_in(lmb_ctx *ctx, const DWPolicy &, Field<PS, NC> &f, const void *src, cudaStream_t st) {
+  const unsigned grid = grid_for(ctx->g.V * ctx->dw_L5, 256);
+  if (ctx->dtype == LMB_DTYPE_C128)
+    pack_field5_kernel<double2, PS, NC><<<grid, 256, 0, st>>>(f, (const double2 *)src, ctx->g, ctx->pd, ctx->dw_L5);
+  else
+    pack_field5_kernel<float2, PS, NC><<<grid, 256, 0, st>>>(f, (const float2 *)src, ctx->g, ctx->pd, ctx->dw_L5);
+  LMB_CHECK_LAUNCH(ctx);
+  return LMB_OK;
+}
+template <int PS, int NC>
+int op_unpack_out(lmb_ctx *ctx, const DWPolicy &, void *dst, const Field<PS, NC> &f, cudaStream_t st) {
+  const unsigned grid = grid_for(ctx->g.V * ctx->dw_L5, 256);
+  if (ctx->dtype == LMB_DTYPE_C128)
+    unpack_field5_kernel<double2, PS, NC><<<grid, 256, 0, st>>>((double2 *)dst, f, ctx->g, ctx->pd, ctx->dw_L5);
+  else
+    unpack_field5_kernel<float2, PS, NC><<<grid, 256, 0, st>>>((float2 *)dst, f, ctx->g, ctx->pd, ctx->dw_L5);
+  LMB_CHECK_LAUNCH(ctx);
+  return LMB_OK;
+}
+
 template <int PS, class Op>
 int apply_generic(lmb_ctx *ctx, const Op &op, void *out, const void *in, int dagger, cudaStream_t st) {
   constexpr int NC = Op::NC;
+  const int64_t V = op_volume(ctx, op);
   Field<PS, NC> fin, fout;
-  if (!make_field(ctx, "apply_in", fin) || !make_field(ctx, "apply_out", fout))
+  if (!make_field(ctx, "apply_in", fin, V) || !make_field(ctx, "apply_out", fout, V))
     return fail(ctx, LMB_ERR_CUDA, "out of device memory (apply workspaces)");
-  int rc = pack_in(ctx, fin, in, st);
+  int rc = op_pack_in(ctx, op, fin, in, st);
   if (rc) return rc;
   EpiStore<PS, NC> epi{fout, nullptr};
   rc = op.template launch<PS>(ctx, fin, dagger, epi, st);
   if (rc) return rc;
-  return unpack_out(ctx, out, fout, st);
+  return op_unpack_out(ctx, op, out, fout, st);
 }
 
 template <class Op>
@@ -437,18 +517,18 @@ int cg_run(lmb_ctx *ctx, const lmb_cg_params *prm, const Op &op, void *x_pad, co
            lmb_cg_result *res, cudaStream_t st) {
   constexpr bool mixed = PS != PREC_DOUBLE;
   constexpr int NC = Op::NC;
-  const int64_t V = ctx->g.V;
+  const int64_t V = op_volume(ctx, op);
   int rc;
   long long nl = 0;  // liblmb200 kernels launched by this solve
   Field<PREC_DOUBLE, NC> b64, x64, r64, t64;
-  if (!make_field(ctx, "cg_b", b64) || !make_field(ctx, "cg_x", x64) || !make_field(ctx, "cg_r", r64) ||
-      !make_field(ctx, "cg_t", t64))
+  if (!make_field(ctx, "cg_b", b64, V) || !make_field(ctx, "cg_x", x64, V) || !make_field(ctx, "cg_r", r64, V) ||
+      !make_field(ctx, "cg_t", t64, V))
     return fail(ctx, LMB_ERR_CUDA, "out of device memory (CG FP64 fields)");
   Field<PS, NC> p, rl, tl;
   Field<PX, NC> xl;
-  if (!make_field(ctx, "cg_p", p)) return fail(ctx, LMB_ERR_CUDA, "out of device memory (CG p)");
+  if (!make_field(ctx, "cg_p", p, V)) return fail(ctx, LMB_ERR_CUDA, "out of device memory (CG p)");
   if constexpr (mixed) {
-    if (!make_field(ctx, "cg_rl", rl) || !make_field(ctx, "cg_tl", tl) || !make_field(ctx, "cg_xl", xl))
+    if (!make_field(ctx, "cg_rl", rl, V) || !make_field(ctx, "cg_tl", tl, V) || !make_field(ctx, "cg_xl", xl, V))
       return fail(ctx, LMB_ERR_CUDA, "out of device memory (CG low-precision fields)");
   } else {
     rl = *(Field<PS, NC> *)&r64;
@@ -471,9 +551,9 @@ int cg_run(lmb_ctx *ctx, const lmb_cg_params *prm, const Op &op, void *x_pad, co
   init.maxiter = prm->maxiter;
   init.status = ST_RUNNING;
   LMB_CUDA(ctx, cudaMemcpyAsync(ctx->st_dev, &init, sizeof init, cudaMemcpyHostToDevice, st));
-  rc = pack_in(ctx, b64, b_pad, st);
+  rc = op_pack_in(ctx, op, b64, b_pad, st);
   if (rc) return rc;
-  rc = pack_in(ctx, x64, x_pad, st);
+  rc = op_pack_in(ctx, op, x64, x_pad, st);
   if (rc) return rc;
   nl += 2;
   if constexpr (mixed) {
@@ -587,7 +667,7 @@ int cg_run(lmb_ctx *ctx, const lmb_cg_params *prm, const Op &op, void *x_pad, co
     if (rc) return rc;
   }
   const double rr_true = ctx->st_host->rr_true;
-  rc = unpack_out(ctx, x_pad, x64, st);
+  rc = op_unpack_out(ctx, op, x_pad, x64, st);
   if (rc) return rc;
   nl++;
   LMB_CUDA(ctx, cudaStreamSynchronize(st));
@@ -1428,6 +1508,7 @@ void lmb_destroy(lmb_ctx *ctx) {
   }
   cudaFree(ctx->clover.F);
   cudaFree(ctx->clover.d);
+  cudaFree(ctx->dw_coef);
   cudaFree(ctx->clover.f);
   cudaFree(ctx->clover.h);
   cudaFree(ctx->clover.ht);
@@ -1604,6 +1685,8 @@ int lmb_cg_ddagd(lmb_ctx *ctx, const lmb_cg_params *prm, void *x, const void *b,
     case LMB_OP_HISQ:
       if (!std::isfinite(prm->mass)) return fail(ctx, LMB_ERR_ARG, "mass must be finite");
       return cg_dispatch(ctx, prm, StaggeredPolicy{true, prm->mass, prm->naik_epsilon}, x, b, res, st);
+    case LMB_OP_DOMAINWALL:
+      return cg_dispatch(ctx, prm, DWPolicy{}, x, b, res, st);
     default: return fail(ctx, LMB_ERR_ARG, "unknown operator %d", prm->op);
   }
 }
@@ -1836,6 +1919,41 @@ int lmb_hisq_fermion_force(lmb_ctx *ctx, const void *const U[4], const uint64_t 
   // dS/dU = -2 d/dU Re<chi, D(U) eta> with chi, eta fixed (dSFdU,
   // ext/LatticeMatricesEnzymeExt.jl:387-460)
   return lmb_hisq_link_pullback(ctx, U, naik_epsilon, -2.0, chi, eta, dU, stream);
+}
+
+int lmb_domainwall_set(lmb_ctx *ctx, int L5, double mass, double M, const double *a, const double *b,
+                       const double *c, void *stream) {
+  if (!ctx_ok(ctx)) return LMB_ERR_ARG;
+  if (L5 <= 0) return fail(ctx, LMB_ERR_ARG, "L5 must be positive");
+  if (!a || !b || !c) return fail(ctx, LMB_ERR_ARG, "null coefficient array");
+  if (!std::isfinite(mass) || !std::isfinite(M)) return fail(ctx, LMB_ERR_ARG, "mass and M must be finite");
+  std::vector<double> h(3 * (size_t)L5);
+  for (int s = 0; s < L5; s++) {
+    h[s] = a[s];
+    h[L5 + s] = b[s];
+    h[2 * L5 + s] = c[s];
+  }
+  for (double v : h)
+    if (!std::isfinite(v)) return fail(ctx, LMB_ERR_ARG, "domain-wall coefficients must all be finite");
+  if (ctx->dw_coef_cap < 3 * L5) {
+    cudaFree(ctx->dw_coef);
+    ctx->dw_coef = nullptr;
+    ctx->dw_coef_cap = 0;
+    LMB_CUDA(ctx, cudaMalloc(&ctx->dw_coef, sizeof(double) * 3 * L5));
+    ctx->dw_coef_cap = 3 * L5;
+  }
+  // ordered on the stream after the kernels that read the previous values
+  LMB_CUDA(ctx, cudaMemcpyAsync(ctx->dw_coef, h.data(), sizeof(double) * 3 * L5, cudaMemcpyHostToDevice,
+                                as_stream(stream)));
+  LMB_CUDA(ctx, cudaStreamSynchronize(as_stream(stream)));
+  ctx->dw_L5 = L5;
+  ctx->dw_mass = mass;
+  ctx->dw_M = M;
+  return LMB_OK;
+}
+
+int lmb_domainwall_apply(lmb_ctx *ctx, void *out, const void *in, int dagger, int precision, void *stream) {
+  return apply_dispatch(ctx, DWPolicy{}, out, in, dagger, precision, stream);
 }
 
 int lmb_wilson_clover_link_pullback(lmb_ctx *ctx, const void *const U[4], double kappa, double csw,

@@ -90,6 +90,12 @@ struct lmb_ctx {
   // (environment LMB_ADJ_SITES=0: sites s and s + V/2)
   bool adj_sites = true;
   lmb::LinkSet links[3];
+  // domain-wall operator (lmb_domainwall_set): L5 slices of the 4D geometry,
+  // mass, M and the coefficients a, b, c (3 L5 doubles, device memory)
+  int dw_L5 = 0;
+  double dw_mass = 0.0, dw_M = 0.0;
+  double *dw_coef = nullptr;
+  int dw_coef_cap = 0;
   lmb::CloverCache clover;
   std::map<std::string, std::pair<void *, size_t>> buffers;
   double *partials = nullptr;
@@ -154,9 +160,10 @@ inline bool ensure_partials(lmb_ctx *ctx, size_t blocks, int nval) {
   return true;
 }
 
+// a field of V sites (default: the context's 4D volume)
 template <int P, int NC>
-inline bool make_field(lmb_ctx *ctx, const std::string &name, Field<P, NC> &f) {
-  const int64_t V = ctx->g.V;
+inline bool make_field(lmb_ctx *ctx, const std::string &name, Field<P, NC> &f, int64_t V = -1) {
+  if (V < 0) V = ctx->g.V;
   f.V = V;
   const size_t nb = Field<P, NC>::bytes(V), mb = Field<P, NC>::norm_bytes(V);
   void *p = workspace(ctx, name, nb + mb + 256);

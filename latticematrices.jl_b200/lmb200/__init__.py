@@ -5,7 +5,7 @@ include/lmb200.h).  Julia names map as `mul!` -> `mul_`, `cg!` -> `cg_`,
 `solve!` -> `solve_`, `update_clover!` -> `update_clover_`, `D'` ->
 `adjoint(D)`.
 """
-from ._lib import ArgumentError, LMBError, load, EXPORTED, LIB_PATH  # noqa: F401
+from ._lib import ArgumentError, DimensionMismatch, LMBError, load, EXPORTED, LIB_PATH  # noqa: F401
 from .lattice import (LatticeMatrix, clear_matrix_, halo_is_dirty,  # noqa: F401
                       mark_halo_dirty_, similar, substitute_)
 from .operators import (CloverFieldStrength4D, WilsonDiracCloverOperator4D,  # noqa: F401
@@ -20,6 +20,8 @@ from .hisq import (HISQDiracCache4D, hisq_fat7_level1_,  # noqa: F401
                    hisq_project_u3_, mul_cached_hisq_,
                    mul_cached_hisq_adjoint_)
 from .clover import wilson_clover_fermion_force_, wilson_clover_link_pullback_  # noqa: F401
+from .domainwall import (D5DW_GeneralizedDomainwallOperator5D,  # noqa: F401
+                         D5DW_MobiusDomainwallOperator5D)
 from .inputs import gaussian_fermion, random_su3_links  # noqa: F401
 from .solver import (CGResult, DdagDOp, cg_, cg_batched_, dot,  # noqa: F401
                      pseudofermion_action, solve_)

@@ -22,7 +22,7 @@ LMB_ERR_UNSUPPORTED = -4
 
 DTYPE_C128, DTYPE_C64 = 0, 1
 PREC = {"double": 0, "single": 1, "half": 2}
-OP_WILSON, OP_WILSON_CLOVER, OP_STAGGERED, OP_HISQ = 0, 1, 2, 3
+OP_WILSON, OP_WILSON_CLOVER, OP_STAGGERED, OP_HISQ, OP_DOMAINWALL = 0, 1, 2, 3, 4
 LINKS_THIN, LINKS_FAT, LINKS_LONG = 0, 1, 2
 CG_REASONS = ("converged", "maximum_iterations", "nonpositive_curvature",
               "numerical_breakdown")
@@ -38,11 +38,16 @@ EXPORTED = (
     "lmb_hisq_links_from_thin", "lmb_cg_ddagd_batched",
     "lmb_hisq_link_pullback", "lmb_hisq_fermion_force",
     "lmb_wilson_clover_link_pullback", "lmb_wilson_clover_fermion_force",
+    "lmb_domainwall_set", "lmb_domainwall_apply",
 )
 
 
 class ArgumentError(ValueError):
     """Validation failure; the reference raises Julia's ArgumentError."""
+
+
+class DimensionMismatch(ArgumentError):
+    """Length mismatch; the reference raises Julia's DimensionMismatch."""
 
 
 class LMBError(RuntimeError):
@@ -154,6 +159,11 @@ def load(path: str = LIB_PATH):
             vp, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_uint64),
             ctypes.c_double, ctypes.c_double, vp, ctypes.POINTER(vp),
             ctypes.POINTER(CGParams), ctypes.POINTER(CGResultC), vp]
+        lib.lmb_domainwall_set.argtypes = [
+            vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, dp, dp, dp,
+            vp]
+        lib.lmb_domainwall_apply.argtypes = [vp, vp, vp, ctypes.c_int,
+                                             ctypes.c_int, vp]
         lib.lmb_hisq_links_from_thin.argtypes = [
             vp, pvp, ctypes.POINTER(ctypes.c_uint64), ctypes.c_double, pvp,
             pvp, vp]

@@ -1,4 +1,4 @@
-"""LatticeMatrix: a halo-padded 4D field in device memory.
+"""LatticeMatrix: a halo-padded 4D (or 5D domain-wall) field in device memory.
 
 Mirrors the reference container LatticeMatrix_standard
 (LatticeMatrices_core.jl:159-184, constructors :297-461): element (ic, jc) of
@@ -6,7 +6,9 @@ site (x, y, z, t) sits at column-major position
 (ic, jc, x+nw, y+nw, z+nw, t+nw) of an (NC1, NC2, X+2nw, Y+2nw, Z+2nw, T+2nw)
 complex array.  The storage is a torch tensor of the reversed shape, so its
 bytes are exactly the bytes of the CuArray behind a Julia LatticeMatrix, and
-its data pointer is what the C ABI receives.
+its data pointer is what the C ABI receives.  A 5D field (domain-wall
+fermions, DiracOperators_5D.jl) adds the fifth coordinate s as the slowest
+index: (NC1, NC2, X+2nw, .., T+2nw, L5+2nw).
 
 Single-rank only (PEs = (1,1,1,1)): the halo is never filled, because the
 kernels wrap periodically with the fermion phase; `halo_epoch` still tracks
@@ -33,13 +35,17 @@ class HaloEpoch:
 class LatticeMatrix:
     """`LatticeMatrix(NC1, NC2, dim, gsize, PEs; nw, elementtype, phases)`."""
 
-    def __init__(self, NC1, NC2, dim, gsize, PEs=(1, 1, 1, 1), *, nw=1,
+    def __init__(self, NC1, NC2, dim, gsize, PEs=None, *, nw=1,
                  elementtype=np.complex128, phases=None, device="cuda"):
         # validation follows LatticeMatrices_core.jl:315-343
+        if PEs is None:
+            PEs = (1,) * dim
         if nw < 0:
             raise ArgumentError(f"nw must be non-negative, got {nw}")
-        if dim != 4:
-            raise ArgumentError("the B200 path handles four-dimensional lattices")
+        if dim not in (4, 5):
+            raise ArgumentError(
+                "the B200 path handles four-dimensional lattices and "
+                "five-dimensional domain-wall fields")
         gsize = tuple(int(v) for v in gsize)
         if len(gsize) != dim:
             raise ArgumentError(
@@ -78,8 +84,8 @@ class LatticeMatrix:
         self.nw = int(nw)
         self.phases = tuple(phases)
         self.elementtype = dt
-        self.coords = (0, 0, 0, 0)
-        self.dims = (1, 1, 1, 1)
+        self.coords = (0,) * dim
+        self.dims = (1,) * dim
         self.halo_epoch = HaloEpoch()
         padded = tuple(v + 2 * self.nw for v in gsize)
         tdt = torch.complex128 if dt == np.complex128 else torch.complex64
@@ -88,10 +94,12 @@ class LatticeMatrix:
 
     # -- construction from a host array (LatticeMatrices_core.jl:405-461) --
     @classmethod
-    def from_array(cls, A, dim=4, PEs=(1, 1, 1, 1), *, nw=1, phases=None,
+    def from_array(cls, A, dim=4, PEs=None, *, nw=1, phases=None,
                    device="cuda"):
         A = np.asarray(A)
         NC1, NC2 = A.shape[:2]
+        if PEs is None:
+            PEs = (1,) * dim
         lm = cls(NC1, NC2, dim, A.shape[2:], PEs, nw=nw,
                  elementtype=A.dtype, phases=phases, device=device)
         lm.set_core(A)
@@ -106,8 +114,7 @@ class LatticeMatrix:
 
     def core_view(self):
         n = self.nw
-        X, Y, Z, T = self.gsize
-        return self.A[n:n + T, n:n + Z, n:n + Y, n:n + X]
+        return self.A[tuple(slice(n, n + v) for v in self.gsize[::-1])]
 
     def set_core(self, A):
         import torch
@@ -121,7 +128,7 @@ class LatticeMatrix:
         mark_halo_dirty_(self)
 
     def gather_matrix(self):
-        """Core values as a Fortran-ordered (NC1, NC2, X, Y, Z, T) array
+        """Core values as a Fortran-ordered (NC1, NC2, X, Y, Z, T[, L5]) array
         (gather_matrix, LatticeMatrices_core.jl:936-993)."""
         return np.asfortranarray(self.core_view().cpu().numpy().T)
 
@@ -132,8 +139,8 @@ class LatticeMatrix:
                              device=self.A.device)
 
     def same_geometry(self, other) -> bool:
-        return (self.gsize == other.gsize and self.nw == other.nw and
-                self.dims == other.dims)
+        return (self.dim == other.dim and self.gsize == other.gsize and
+                self.nw == other.nw and self.dims == other.dims)
 
 
 def mark_halo_dirty_(ls: LatticeMatrix):

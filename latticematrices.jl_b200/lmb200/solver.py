@@ -17,7 +17,8 @@ from dataclasses import dataclass
 import numpy as np
 
 from ._lib import (ArgumentError, CG_REASONS, CGParams, CGResultC, PREC,
-                   OP_HISQ, OP_STAGGERED, OP_WILSON, OP_WILSON_CLOVER)
+                   OP_DOMAINWALL, OP_HISQ, OP_STAGGERED, OP_WILSON,
+                   OP_WILSON_CLOVER)
 from .lattice import LatticeMatrix, mark_halo_dirty_
 from .operators import (HISQDiracOperator4D, StaggeredDiracOperator4D,
                         WilsonDiracCloverOperator4D, WilsonDiracOperator4D,
@@ -99,6 +100,9 @@ def _native_operator(A):
     from .hisq import HISQDiracCache4D
     if isinstance(D, HISQDiracCache4D):
         return D, OP_HISQ
+    from .domainwall import _DomainwallBase
+    if isinstance(D, _DomainwallBase):
+        return D, OP_DOMAINWALL
     return None
 
 
@@ -125,6 +129,8 @@ def cg_(x, A, b, r=None, p=None, Ap=None, *, rtol=1e-10, atol=0.0,
         prm.check_interval = int(check_interval)
         prm.profile = int(bool(profile))
         st = _stream()
+        if op == OP_DOMAINWALL:
+            D._validate(x, b)
         ctx = binder._bind(b, st)
         res = CGResultC()
         ctx.check(ctx.lib.lmb_cg_ddagd(ctx.handle, ctypes.byref(prm),

@@ -94,3 +94,50 @@ def test_cg_validation_before_cuda():
     D = lmb.DdagDOp(None, b)
     with pytest.raises(lmb.ArgumentError, match="alias"):
         D.mul_(x, b)
+
+
+def test_domainwall_validation_before_cuda():
+    """Constructor and application checks of DiracOperators_5D.jl:15-21,
+    66-91 and _require_5d_halo (:155-159), raised before any CUDA call."""
+    import lmb200 as lmb
+    U = [_cpu_field(lmb, 3, 3) for _ in range(4)]
+    L5 = 3
+    psi = lmb.LatticeMatrix(3, 4, 5, (4, 4, 4, 4, L5), device="cpu")
+    out = psi.similar()
+    assert out.dim == 5 and out.gsize == (4, 4, 4, 4, L5)
+    # 5D storage: the fifth coordinate is the slowest padded index
+    arr = np.asfortranarray(np.random.default_rng(1).normal(size=(3, 4, 4, 4, 4, 4, L5)) + 0j)
+    psi.set_core(arr)
+    assert np.array_equal(psi.gather_matrix(), arr)
+    assert psi.A.numpy()[1 + 2, 1 + 0, 1 + 3, 1 + 1, 1 + 2, 3, 2] == arr[2, 3, 2, 1, 3, 0, 2]
+    with pytest.raises(lmb.ArgumentError, match="four gauge links"):
+        lmb.D5DW_MobiusDomainwallOperator5D(U[:3], L5, 0.1, -1.8, 2.0, 1.0)
+    with pytest.raises(lmb.ArgumentError, match="integer"):
+        lmb.D5DW_MobiusDomainwallOperator5D(U, 3.0, 0.1, -1.8, 2.0, 1.0)
+    with pytest.raises(lmb.ArgumentError, match="positive"):
+        lmb.D5DW_MobiusDomainwallOperator5D(U, 0, 0.1, -1.8, 2.0, 1.0)
+    with pytest.raises(lmb.DimensionMismatch, match="length L5"):
+        lmb.D5DW_GeneralizedDomainwallOperator5D(U, L5, 0.1, -1.8, [1] * 3, [1] * 2, [0] * 3)
+    with pytest.raises(lmb.ArgumentError, match="finite"):
+        lmb.D5DW_GeneralizedDomainwallOperator5D(U, L5, 0.1, -1.8, [1] * 3, [1, np.nan, 1], [0] * 3)
+    D = lmb.D5DW_GeneralizedDomainwallOperator5D(U, L5, 0.1, -1.8, [1] * 3, [1.5] * 3, [0.5] * 3)
+    assert D.kappa_wilson == pytest.approx(1 / (8 - 3.6))
+    M = lmb.D5DW_MobiusDomainwallOperator5D(U, L5, 0.1, -1.8, 2.0, 1.0)
+    a, b, c = M.abc()
+    assert list(a) == [1.0] * L5 and list(b) == [1.5] * L5 and list(c) == [0.5] * L5
+    assert lmb.adjoint(lmb.adjoint(D)) is D
+    with pytest.raises(lmb.ArgumentError, match="distinct"):
+        lmb.mul_(psi, D, psi)
+    with pytest.raises(lmb.ArgumentError, match="five-dimensional"):
+        lmb.mul_(_cpu_field(lmb, 3, 4), D, _cpu_field(lmb, 3, 4))
+    with pytest.raises(lmb.DimensionMismatch, match="fifth extent"):
+        wrong = lmb.LatticeMatrix(3, 4, 5, (4, 4, 4, 4, 2), device="cpu")
+        lmb.mul_(wrong.similar(), D, wrong)
+    flat = lmb.LatticeMatrix(3, 4, 5, (4, 4, 4, 4, L5), nw=0, device="cpu")
+    with pytest.raises(lmb.ArgumentError, match="nw=0"):
+        lmb.mul_(flat.similar(), D, flat)
+    other = lmb.LatticeMatrix(3, 4, 5, (4, 4, 2, 4, L5), device="cpu")
+    with pytest.raises(lmb.ArgumentError, match="geometry"):
+        lmb.mul_(other.similar(), D, other)
+    with pytest.raises(lmb.ArgumentError, match="distinct|alias"):
+        lmb.cg_(psi, lmb.DdagDOp(D, out), psi)
