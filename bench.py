@@ -94,13 +94,15 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
     ap.add_argument("--workload", default="clover",
-                    choices=["clover", "wilson8", "hisq", "batched", "force", "clover_force"],
+                    choices=["clover", "wilson8", "hisq", "batched", "force", "clover_force", "dw"],
                     help="clover: 32^3x64 Wilson-clover mixed vs FP64 CG (the "
                          "headline line); wilson8: 8^4 Wilson FP64 CG beside the "
                          "CPU oracle; hisq: 48^3x96 HISQ smearing + CG; batched: "
                          "multi-RHS multi-lattice Wilson CG; force: 24^4 HISQ "
                          "fermion force with a finite-difference check; "
-                         "clover_force: 24^4 Wilson-clover fermion force, same check")
+                         "clover_force: 24^4 Wilson-clover fermion force, same check; "
+                         "dw: 16^3x32 x L5 12 Mobius domain-wall D5'D5 CG")
+    ap.add_argument("--l5", type=int, default=12)
     ap.add_argument("--fd-directions", type=int, default=64)
     return ap.parse_args()
 
@@ -734,6 +736,65 @@ def run_clover_force(args):
           flush=True)
 
 
+def run_dw(args):
+    """Mobius domain-wall D5^+ D5 CG (DiracOperators_5D.jl; the Mobius
+    example of benchmark/ddagd_cg/README.md): 16^3x32, L5 12, mass 0.1,
+    M -1, b 2, c 1, links exp(0.2 i H) seed 1, unit complex Gaussian 5D
+    source (torch generator seed 2), phases (1,1,1,-1); FP64 CG and the FP32
+    / int16 inner solves with FP64 reliable updates, each to FP64 true
+    residual 1e-10, zero start."""
+    import contextlib
+    import torch
+    import lmb200 as lmb
+    L = tuple(int(v) for v in (args.lattice if args.lattice != "32,32,32,64"
+                                else "16,16,16,32").split(","))
+    L5 = args.l5
+    V5 = L[0] * L[1] * L[2] * L[3] * L5
+    U = lmb.random_su3_links(L, 0.2, 1)
+    with contextlib.redirect_stdout(sys.stderr):
+        D = lmb.D5DW_MobiusDomainwallOperator5D(U, L5, 0.1, -1.0, 2.0, 1.0)
+    b = lmb.LatticeMatrix(3, 4, 5, L + (L5,), phases=PHASES + (1,))
+    g = torch.Generator(device="cuda").manual_seed(2)
+    b.core_view().copy_(torch.randn(b.core_view().shape, dtype=torch.complex128,
+                                    device="cuda", generator=g))
+    lmb.mark_halo_dirty_(b)
+    A = lmb.DdagDOp(D, b.similar())
+    x = b.similar()
+    st = torch.cuda.current_stream()
+    bn = float(torch.linalg.vector_norm(b.core_view()))
+    out = {"workload": "Mobius DW D5'D5 CG %dx%dx%dx%d x L5 %d, m 0.1, M -1, b 2, c 1" % (L + (L5,))}
+    for prec in ("double", "single", "half"):
+        lmb.clear_matrix_(x)
+        lmb.cg_(x, A, b, rtol=args.rtol, precision=prec, maxiter=args.maxiter)
+        lmb.clear_matrix_(x)
+        res, t = _timed(lambda: lmb.cg_(x, A, b, rtol=args.rtol, precision=prec,
+                                         maxiter=args.maxiter, profile=True), st)
+        k1 = res.dslash_ms / max(res.dslash_launches, 1)
+        k2 = res.update_ms / max(res.update_launches, 1)
+        sp, xb = spinor_bytes(prec), x_bytes(prec)
+        links = 4 * res.link_reals * REAL_BYTES[prec] / L5  # 4D links shared by L5 slices
+        # bytes per 5D site the two-pass kernels move (each operand once):
+        #  K1 = D5 p:  Y = B p + C F p (p, Y), stencil (Y, p, out, links)
+        #  K2 = D5^+ t + CG update: stencil (t, Z, links), local (t, Z, p,
+        #       r rw, x rw)
+        k1_b = 5 * sp + links
+        k2_b = 7 * sp + 2 * xb + links
+        # the operator's compulsory bytes (a one-pass kernel): in, out, links
+        k1_min = 2 * sp + links
+        k2_min = 4 * sp + 2 * xb + links
+        out[prec] = {"time_s": t, "iterations": res.iterations, "converged": res.converged,
+                     "true_rel_residual": res.true_residual_norm / bn,
+                     "reliable_updates": res.reliable_updates,
+                     "k1_ms": k1, "k1_gbs": k1_b * V5 / (k1 * 1e-3) / 1e9,
+                     "k1_gbs_compulsory": k1_min * V5 / (k1 * 1e-3) / 1e9,
+                     "k2_ms": k2, "k2_gbs": k2_b * V5 / (k2 * 1e-3) / 1e9,
+                     "k2_gbs_compulsory": k2_min * V5 / (k2 * 1e-3) / 1e9}
+    for prec in ("single", "half"):
+        out["speedup_%s_vs_fp64" % prec] = out["double"]["time_s"] / out[prec]["time_s"]
+    out["hbm_peak_gbs"] = measured_peak()[0]
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -744,7 +805,7 @@ def main():
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         {"wilson8": run_wilson8, "hisq": run_hisq, "batched": run_batched,
-         "force": run_force, "clover_force": run_clover_force}[args.workload](args)
+         "force": run_force, "clover_force": run_clover_force, "dw": run_dw}[args.workload](args)
 
 
 if __name__ == "__main__":
