@@ -357,6 +357,14 @@ struct DWPolicy {
     if (rc) return rc;
     return ensure_link_precision(ctx, ctx->links[LMB_LINKS_THIN], prec, st);
   }
+  static bool one_pass(const lmb_ctx *ctx) { return ctx->dw_L5 <= kDslashThreads && !ctx->dw_two_pass; }
+  // blocks of the largest launch (the one-pass adjoint holds whole 4D points)
+  static int64_t max_blocks(const lmb_ctx *ctx) {
+    const int64_t flat = grid_for(ctx->g.V * ctx->dw_L5, kDslashThreads);
+    if (!one_pass(ctx)) return flat;
+    const int64_t pts = grid_for(ctx->g.V, kDslashThreads / ctx->dw_L5);
+    return pts > flat ? pts : flat;
+  }
   DWParams params(const lmb_ctx *ctx) const {
     const int L5 = ctx->dw_L5;
     return DWParams{L5, ctx->dw_mass, ctx->dw_M, ctx->dw_coef, ctx->dw_coef + L5, ctx->dw_coef + 2 * L5};
@@ -370,6 +378,16 @@ struct DWPolicy {
       return fail(ctx, LMB_ERR_CUDA, "out of device memory (domain-wall workspace)");
     const DWParams d = params(ctx);
     const unsigned grid = grid_for(V5, kDslashThreads);
+    if (one_pass(ctx)) {
+      if (!dagger) {
+        dw_forward_kernel<R><<<grid, kDslashThreads, 0, st>>>(ctx->g, in, U, d, epi);
+      } else {
+        const int npts = kDslashThreads / d.L5;
+        dw_adjoint_kernel<R><<<grid_for(V4, npts), kDslashThreads, 0, st>>>(ctx->g, in, U, d, npts, epi);
+      }
+      LMB_CHECK_LAUNCH(ctx);
+      return LMB_OK;
+    }
     if (!dagger) {
       dw_fifth_kernel<P><<<grid, kDslashThreads, 0, st>>>(tmp, in, V4, d, epi);
       dw_stencil_kernel<R, 0, 1><<<grid, kDslashThreads, 0, st>>>(ctx->g, tmp, in, U, d, epi);
@@ -414,6 +432,10 @@ int unpack_out(lmb_ctx *ctx, void *dst, const Field<PS, NC> &f, cudaStream_t st)
 
 // operator hooks with the 4D defaults: field volume, pack, unpack
 template <class Op> int64_t op_volume(const lmb_ctx *ctx, const Op &) { return ctx->g.V; }
+// reduction partials a CG stencil launch of the operator needs (one per block)
+template <class Op> int64_t op_max_blocks(const lmb_ctx *ctx, const Op &op) {
+  return grid_for(op_volume(ctx, op), kDslashThreads);
+}
 template <class Op, int PS, int NC>
 int op_pack_in(lmb_ctx *ctx, const Op &, Field<PS, NC> &f, const void *src, cudaStream_t st) {
   return pack_in(ctx, f, src, st);
@@ -424,6 +446,7 @@ int op_unpack_out(lmb_ctx *ctx, const Op &, void *dst, const Field<PS, NC> &f, c
 }
 
 inline int64_t op_volume(const lmb_ctx *ctx, const DWPolicy &) { return ctx->g.V * ctx->dw_L5; }
+inline int64_t op_max_blocks(const lmb_ctx *ctx, const DWPolicy &) { return DWPolicy::max_blocks(ctx); }
 template <int PS, int NC>
 int op_pack_in(lmb_ctx *ctx, const DWPolicy &, Field<PS, NC> &f, const void *src, cudaStream_t st) {
   const unsigned grid = grid_for(ctx->g.V * ctx->dw_L5, 256);
@@ -536,7 +559,10 @@ int cg_run(lmb_ctx *ctx, const lmb_cg_params *prm, const Op &op, void *x_pad, co
     xl = *(Field<PX, NC> *)&x64;
   }
   const unsigned dgrid = grid_for(V, kDslashThreads), bgrid = grid_for(V, kBlasThreads);
-  if (!ensure_partials(ctx, dgrid > bgrid ? dgrid : bgrid, 2))
+  const int64_t ogrid = op_max_blocks(ctx, op);
+  int64_t pgrid = dgrid > bgrid ? dgrid : bgrid;
+  if (ogrid > pgrid) pgrid = ogrid;
+  if (!ensure_partials(ctx, pgrid, 2))
     return fail(ctx, LMB_ERR_CUDA, "out of device memory (reduction partials)");
   rc = op.prepare(ctx, PREC_DOUBLE, st);
   if (rc) return rc;
@@ -1479,6 +1505,7 @@ lmb_ctx *lmb_create(int device) {
   ctx->device = device;
   if (const char *ps = getenv("LMB_PAIR_SITES")) ctx->pair_sites = atoi(ps) != 0;
   if (const char *as = getenv("LMB_ADJ_SITES")) ctx->adj_sites = atoi(as) != 0;
+  if (const char *dw = getenv("LMB_DW_TWO_PASS")) ctx->dw_two_pass = atoi(dw) != 0;
   if (cudaMalloc(&ctx->counter, sizeof(unsigned)) != cudaSuccess ||
       cudaMemset(ctx->counter, 0, sizeof(unsigned)) != cudaSuccess ||
       cudaMalloc(&ctx->st_dev, sizeof(CGState)) != cudaSuccess ||

@@ -96,6 +96,9 @@ struct lmb_ctx {
   double dw_mass = 0.0, dw_M = 0.0;
   double *dw_coef = nullptr;
   int dw_coef_cap = 0;
+  // LMB_DW_TWO_PASS=1 in the environment: domain-wall applications in two
+  // passes (a local pass and a stencil pass) at every L5, instead of one
+  bool dw_two_pass = false;
   lmb::CloverCache clover;
   std::map<std::string, std::pair<void *, size_t>> buffers;
   double *partials = nullptr;

@@ -155,3 +155,33 @@ def test_cg_generalized_edge_cases(lmb, orc):
     assert few.reason == "maximum_iterations" and few.iterations == 2
     res = lmb.cg_(bd.similar(), A, bd, rtol=1e-11)
     assert res.converged
+
+
+@pytest.mark.parametrize("dagger", [False, True])
+def test_two_pass_kernels_match_oracle(lmb, orc, monkeypatch, dagger):
+    """LMB_DW_TWO_PASS=1 (read when the context is created) selects the
+    two-pass kernels; L5 > 128 takes them in any case."""
+    monkeypatch.setenv("LMB_DW_TWO_PASS", "1")
+    for L, L5 in (((4, 4, 2, 4), 5), ((2, 2, 2, 2), 130)):
+        U, psi, Ud, pd = _fields(lmb, orc, L, L5, phases=TWISTED, seed=17)
+        a, b, c = _general(L5, 19)
+        D = lmb.D5DW_GeneralizedDomainwallOperator5D(Ud, L5, 0.05, -1.2, a, b, c)
+        for prec, bar in (("double", 1e-13), ("single", 5e-6)):
+            out = pd.similar()
+            lmb.mul_(out, lmb.adjoint(D) if dagger else D, pd, precision=prec)
+            ref = orc.domainwall(U, psi, 0.05, -1.2, a, b, c, TWISTED, dagger=dagger)
+            assert rd.rel_err(out.gather_matrix(), ref) <= bar
+
+
+def test_long_fifth_dimension_cg(lmb, orc):
+    """L5 = 130 > 128: two-pass kernels inside the CG driver."""
+    L, L5 = (2, 2, 2, 4), 130
+    U, b, Ud, bd = _fields(lmb, orc, L, L5, seed=23)
+    D = lmb.D5DW_MobiusDomainwallOperator5D(Ud, L5, 0.2, -1.5, 1.5, 0.5)
+    x = bd.similar()
+    res = lmb.cg_(x, lmb.DdagDOp(D, bd.similar()), bd, rtol=1e-10, precision="half")
+    assert res.converged
+    a, bb, c = orc.mobius_coefficients(L5, 1.5, 0.5)
+    xs = x.gather_matrix()
+    true_rel = np.linalg.norm(b - _ddagd(orc, U, xs, 0.2, -1.5, a, bb, c)) / np.linalg.norm(b)
+    assert true_rel <= 1.05e-10
