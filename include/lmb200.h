@@ -243,6 +243,21 @@ int lmb_wilson_clover_fermion_force(lmb_ctx *ctx, const void *const U[4],
  * 392-399). */
 int lmb_clover_field_strength(lmb_ctx *ctx, void *const F[6], void *stream);
 
+/* Solve D x = b for the Wilson or Wilson-clover operator (params->op,
+ * kappa, csw) by even/odd (Schur) preconditioning: the even half lattice
+ * carries Dh = A_ee - kappa^2 H_eo A_oo^-1 H_oe, solved by CG on Dh Dh^+
+ * (CGNE) with the CG driver of lmb_cg_ddagd (FP64, or FP32 / int16 inner
+ * iterations with FP64 reliable updates), then x_o = A_oo^-1 (b_o +
+ * kappa H_oe x_e).  Parity as the reference's even/odd kernels
+ * (_global_site_is_even, LatticeMatrices.jl:357-363; linearalgebra_D.jl:
+ * 2815-2930).  The reference reaches D x = b as cg!(x, DdagDOp(D), D'b);
+ * this entry stops on the FP64 residual of D x = b itself:
+ * |b - D x| <= max(atol, rtol |b|), reported in result->true_residual_norm.
+ * All lattice extents must be even; x's initial content is ignored (zero
+ * start).  Synchronises the stream. */
+int lmb_solve_evenodd(lmb_ctx *ctx, const lmb_cg_params *params, void *x,
+                      const void *b, lmb_cg_result *result, void *stream);
+
 /* cg!(x, DdagDOp(D, temp), b, r, p, Ap; rtol, atol, maxiter)
  * (LinearAlgebras/cg.jl:73-137, Operators/DiracOperators.jl:93-143,
  * benchmark/ddagd_cg/ddagd_cg.jl:587-644).  x holds the initial guess on entry

@@ -49,6 +49,7 @@ struct CloverCache {
   float scale = 1.f;
   bool d_valid = false;
   uint64_t f_version = ~0ull, h_version = ~0ull, d_version = 0;
+  uint64_t src_version = ~0ull;  // inverse blocks: d_version of the blocks inverted
 };
 
 }  // namespace lmb
@@ -100,6 +101,7 @@ struct lmb_ctx {
   // passes (a local pass and a stencil pass) at every L5, instead of one
   bool dw_two_pass = false;
   lmb::CloverCache clover;
+  lmb::CloverCache clover_inv;  // A^-1 blocks (even/odd solve)
   std::map<std::string, std::pair<void *, size_t>> buffers;
   double *partials = nullptr;
   size_t partials_cap = 0;

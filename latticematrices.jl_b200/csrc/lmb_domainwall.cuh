@@ -304,17 +304,6 @@ __global__ void __launch_bounds__(kDslashThreads, DWMinBlocks<R>::value)
 // ---------------------------------------------------------------------------
 // two-pass kernels (any L5)
 // ---------------------------------------------------------------------------
-// a store that skips with another epilogue (a paused CG skips every pass)
-template <int PS, class Follow>
-struct EpiStoreFollow {
-  Field<PS, 12> out;
-  Follow follow;
-  LMB_D bool skip() const { return follow.skip(); }
-  template <typename R> LMB_D void operator()(int s, bool active, const Cx<R> *v) const {
-    if (active) out.store(s, v);
-  }
-};
-
 // D5 pass 1: Y = b psi + c F psi
 template <int P, class Epi>
 __global__ void __launch_bounds__(kDslashThreads)

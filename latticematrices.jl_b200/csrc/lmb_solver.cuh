@@ -252,6 +252,41 @@ struct EpiCGUpdate {  // K2
   }
 };
 
+// the first pass of a two-pass operator: a plain store that skips whenever
+// the epilogue of the second pass does (a paused CG skips every pass)
+template <int PS, class Follow>
+struct EpiStoreFollow {
+  Field<PS, 12> out;
+  Follow follow;
+  LMB_D bool skip() const { return follow.skip(); }
+  template <typename R> LMB_D void operator()(int s, bool active, const Cx<R> *v) const {
+    if (active) out.store(s, v);
+  }
+};
+
+// |b - v|^2 summed over the grid into *out (no CG state)
+template <int NC = 12>
+struct EpiResidualNorm {
+  Field<PREC_DOUBLE, NC> b;
+  double *partials;
+  unsigned *counter;
+  double *out;
+  LMB_D bool skip() const { return false; }
+  template <typename R> LMB_D void operator()(int s, bool active, const Cx<R> *v) const {
+    double n2[1] = {0.0}, tot[1];
+    if (active) {
+      Cx<double> bv[NC];
+      b.load(s, bv);
+#pragma unroll
+      for (int k = 0; k < NC; k++) {
+        const double dr = bv[k].re - (double)v[k].re, di = bv[k].im - (double)v[k].im;
+        n2[0] += dr * dr + di * di;
+      }
+    }
+    if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0) *out = tot[0];
+  }
+};
+
 // r = b - v (FP64), r_low = r (optional), |r|^2 -> finalize_true(mode)
 template <int PS, int NC = 12>
 struct EpiTrueResidual {

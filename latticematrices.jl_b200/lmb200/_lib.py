@@ -38,7 +38,7 @@ EXPORTED = (
     "lmb_hisq_links_from_thin", "lmb_cg_ddagd_batched",
     "lmb_hisq_link_pullback", "lmb_hisq_fermion_force",
     "lmb_wilson_clover_link_pullback", "lmb_wilson_clover_fermion_force",
-    "lmb_domainwall_set", "lmb_domainwall_apply",
+    "lmb_domainwall_set", "lmb_domainwall_apply", "lmb_solve_evenodd",
 )
 
 
@@ -169,6 +169,8 @@ def load(path: str = LIB_PATH):
             pvp, vp]
         lib.lmb_cg_ddagd.argtypes = [vp, ctypes.POINTER(CGParams), vp, vp,
                                      ctypes.POINTER(CGResultC), vp]
+        lib.lmb_solve_evenodd.argtypes = [vp, ctypes.POINTER(CGParams), vp,
+                                          vp, ctypes.POINTER(CGResultC), vp]
         lib.lmb_field_dot.argtypes = [vp, vp, vp, ctypes.c_int, dp, vp]
         lib.lmb_random_su3_links.argtypes = [vp, ctypes.POINTER(vp),
                                              ctypes.c_double, ctypes.c_uint64,
