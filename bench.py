@@ -94,14 +94,17 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
     ap.add_argument("--workload", default="clover",
-                    choices=["clover", "wilson8", "hisq", "batched", "force", "clover_force", "dw"],
+                    choices=["clover", "wilson8", "hisq", "batched", "force", "clover_force", "dw",
+                             "evenodd"],
                     help="clover: 32^3x64 Wilson-clover mixed vs FP64 CG (the "
                          "headline line); wilson8: 8^4 Wilson FP64 CG beside the "
                          "CPU oracle; hisq: 48^3x96 HISQ smearing + CG; batched: "
                          "multi-RHS multi-lattice Wilson CG; force: 24^4 HISQ "
                          "fermion force with a finite-difference check; "
                          "clover_force: 24^4 Wilson-clover fermion force, same check; "
-                         "dw: 16^3x32 x L5 12 Mobius domain-wall D5'D5 CG")
+                         "dw: 16^3x32 x L5 12 Mobius domain-wall D5'D5 CG; evenodd: "
+                         "32^3x64 clover D x = b, even/odd Schur solve vs the "
+                         "D'D CG route")
     ap.add_argument("--l5", type=int, default=12)
     ap.add_argument("--fd-directions", type=int, default=64)
     return ap.parse_args()
@@ -795,6 +798,49 @@ def run_dw(args):
     print(json.dumps(out), flush=True)
 
 
+def run_evenodd(args):
+    """D x = b on the headline lattice (32^3x64 Wilson-clover, kappa 0.1355,
+    cSW 1.0, links exp(0.2 i H) seed 1, Gaussian source seed 2): the
+    even/odd Schur solve (solve_evenodd_) against the reference's route to
+    the same x, cg!(x, DdagDOp(D), D'b), both at rtol 1e-10, FP64 and int16
+    inner iterations; every solve's |b - D x| / |b| is recomputed in FP64."""
+    import torch
+    import lmb200 as lmb
+    L = tuple(int(v) for v in args.lattice.split(","))
+    U = lmb.random_su3_links(L, args.amplitude, 1)
+    b = lmb.gaussian_fermion(L, 3, 4, 2, phases=PHASES)
+    D = lmb.WilsonDiracCloverOperator4D(U, args.kappa, args.csw)
+    Db = b.similar()
+    lmb.mul_(Db, lmb.adjoint(D), b)
+    A = lmb.DdagDOp(D, b.similar())
+    x, t = b.similar(), b.similar()
+    st = torch.cuda.current_stream()
+    bn = float(torch.linalg.vector_norm(b.core_view()))
+
+    def rel_residual():
+        lmb.mul_(t, D, x)
+        return float(torch.linalg.vector_norm(b.core_view() - t.core_view())) / bn
+
+    out = {"workload": "Wilson-clover D x = b %dx%dx%dx%d, kappa %g, cSW %g" % (L + (args.kappa, args.csw))}
+    for prec in ("double", "half"):
+        for route in ("evenodd", "ddagd_cg"):
+            if route == "evenodd":
+                solve = lambda: lmb.solve_evenodd_(x, D, b, rtol=args.rtol, precision=prec,
+                                                   maxiter=args.maxiter)
+            else:
+                def solve():
+                    lmb.clear_matrix_(x)
+                    return lmb.cg_(x, A, Db, rtol=args.rtol, precision=prec, maxiter=args.maxiter)
+            solve()
+            res, sec = _timed(solve, st)
+            out["%s_%s" % (route, prec)] = {"time_s": sec, "iterations": res.iterations,
+                                            "converged": res.converged,
+                                            "rel_residual_b_minus_Dx": rel_residual()}
+    for prec in ("double", "half"):
+        out["speedup_%s" % prec] = out["ddagd_cg_%s" % prec]["time_s"] / out["evenodd_%s" % prec]["time_s"]
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -805,7 +851,8 @@ def main():
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         {"wilson8": run_wilson8, "hisq": run_hisq, "batched": run_batched,
-         "force": run_force, "clover_force": run_clover_force, "dw": run_dw}[args.workload](args)
+         "force": run_force, "clover_force": run_clover_force, "dw": run_dw,
+         "evenodd": run_evenodd}[args.workload](args)
 
 
 if __name__ == "__main__":
