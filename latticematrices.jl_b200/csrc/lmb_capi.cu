@@ -504,6 +504,115 @@ int op_unpack_out(lmb_ctx *ctx, const DWPolicy &, void *dst, const Field<PS, NC>
   return LMB_OK;
 }
 
+// parity-ordered copy (eo_permute_kernel) of `nplanes` planes of T at byte
+// offset `off` of buffer `name`, rebuilt when the source version, the volume
+// or the buffer changes (*stale: an earlier region of the buffer was rebuilt)
+template <typename T>
+int eo_copy(lmb_ctx *ctx, const std::string &name, size_t bytes, size_t off, const T *src, int nplanes,
+            uint64_t version, bool *stale, cudaStream_t st) {
+  char *buf = (char *)workspace(ctx, name, bytes);
+  if (!buf) return fail(ctx, LMB_ERR_CUDA, "out of device memory (parity-ordered copy)");
+  auto it = ctx->eo_tags.find(name);
+  if (*stale || it == ctx->eo_tags.end() || it->second.version != version || it->second.V != ctx->g.V ||
+      it->second.ptr != buf) {
+    *stale = true;
+    eo_permute_kernel<T><<<grid_for(ctx->g.V, 256), 256, 0, st>>>((T *)(buf + off), src, nplanes, ctx->g);
+    LMB_CHECK_LAUNCH(ctx);
+  }
+  return LMB_OK;
+}
+void eo_tag(lmb_ctx *ctx, const std::string &name, uint64_t version) {
+  ctx->eo_tags[name] = lmb_ctx::EoTag{version, ctx->g.V, workspace(ctx, name, 0)};
+}
+const char *eo_buffer(lmb_ctx *ctx, const std::string &name) { return (const char *)workspace(ctx, name, 0); }
+
+// parity-ordered links (thin set) and clover blocks in precision prec
+int ensure_eo_copies(lmb_ctx *ctx, int prec, bool clover, cudaStream_t st) {
+  const LinkSet &ls = ctx->links[LMB_LINKS_THIN];
+  const int64_t V = ctx->g.V;
+  const char *tag = prec == PREC_DOUBLE ? "d" : (prec == PREC_SINGLE ? "s" : "h");
+  int rc;
+  bool stale = false;
+  const std::string un = std::string("eo_U_") + tag;
+  if (ls.recon(prec)) {
+    if (prec == PREC_DOUBLE) rc = eo_copy(ctx, un, sizeof(double2) * 24 * V, 0, ls.d12, 24, ls.version, &stale, st);
+    else if (prec == PREC_SINGLE) rc = eo_copy(ctx, un, sizeof(float4) * 12 * V, 0, ls.f12, 12, ls.version, &stale, st);
+    else rc = eo_copy(ctx, un, sizeof(int4) * 6 * V, 0, ls.h12, 6, ls.version, &stale, st);
+  } else {
+    if (prec == PREC_DOUBLE) {
+      rc = eo_copy(ctx, un, sizeof(double2) * 36 * V, 0, ls.d, 36, ls.version, &stale, st);
+    } else if (prec == PREC_SINGLE) {
+      const size_t nb = sizeof(float2) * 36 * V;
+      rc = eo_copy(ctx, un, nb, 0, (const float4 *)ls.f, 16, ls.version, &stale, st);
+      if (!rc)
+        rc = eo_copy(ctx, un, nb, sizeof(float4) * 16 * V, (const float2 *)((const float4 *)ls.f + 16 * V), 4,
+                     ls.version, &stale, st);
+    } else {
+      rc = eo_copy(ctx, un, sizeof(int) * 36 * V, 0, ls.h, 36, ls.version, &stale, st);
+    }
+  }
+  if (rc) return rc;
+  eo_tag(ctx, un, ls.version);
+  if (!clover) return LMB_OK;
+  const CloverCache *caches[2] = {&ctx->clover, &ctx->clover_inv};
+  const char *names[2] = {"eo_A_", "eo_Ai_"};
+  for (int w = 0; w < 2; w++) {
+    const CloverCache &cc = *caches[w];
+    const std::string n = std::string(names[w]) + tag;
+    stale = false;
+    if (prec == PREC_DOUBLE) {
+      rc = eo_copy(ctx, n, sizeof(double2) * 36 * V, 0, cc.d, 36, cc.d_version, &stale, st);
+    } else if (prec == PREC_SINGLE) {
+      rc = eo_copy(ctx, n, sizeof(float4) * 18 * V, 0, cc.f, 18, cc.d_version, &stale, st);
+    } else {
+      const size_t nb = sizeof(int4) * 8 * V + sizeof(int2) * 2 * V;
+      rc = eo_copy(ctx, n, nb, 0, cc.h, 8, cc.d_version, &stale, st);
+      if (!rc) rc = eo_copy(ctx, n, nb, sizeof(int4) * 8 * V, cc.ht, 2, cc.d_version, &stale, st);
+    }
+    if (rc) return rc;
+    eo_tag(ctx, n, cc.d_version);
+  }
+  return LMB_OK;
+}
+
+template <int P> Gauge<P> eo_gauge_view(lmb_ctx *ctx);
+template <> Gauge<PREC_DOUBLE> eo_gauge_view<PREC_DOUBLE>(lmb_ctx *ctx) {
+  return {(const double2 *)eo_buffer(ctx, "eo_U_d"), ctx->g.V, ctx->links[LMB_LINKS_THIN].scale};
+}
+template <> Gauge<PREC_SINGLE> eo_gauge_view<PREC_SINGLE>(lmb_ctx *ctx) {
+  return {(const float4 *)eo_buffer(ctx, "eo_U_s"), ctx->g.V, ctx->links[LMB_LINKS_THIN].scale};
+}
+template <> Gauge<PREC_HALF> eo_gauge_view<PREC_HALF>(lmb_ctx *ctx) {
+  return {(const int *)eo_buffer(ctx, "eo_U_h"), ctx->g.V,
+          base_of_exponent(pow2_exponent(ctx->links[LMB_LINKS_THIN].scale))};
+}
+template <int P> Gauge12<P> eo_gauge12_view(lmb_ctx *ctx);
+template <> Gauge12<PREC_DOUBLE> eo_gauge12_view<PREC_DOUBLE>(lmb_ctx *ctx) {
+  return {(const double2 *)eo_buffer(ctx, "eo_U_d"), ctx->g.V, 1.f};
+}
+template <> Gauge12<PREC_SINGLE> eo_gauge12_view<PREC_SINGLE>(lmb_ctx *ctx) {
+  return {(const float4 *)eo_buffer(ctx, "eo_U_s"), ctx->g.V, 1.f};
+}
+template <> Gauge12<PREC_HALF> eo_gauge12_view<PREC_HALF>(lmb_ctx *ctx) {
+  return {(const int4 *)eo_buffer(ctx, "eo_U_h"), ctx->g.V, 1.f};
+}
+template <int P> Clover<P> eo_clover_view(lmb_ctx *ctx, int inverse);
+template <> Clover<PREC_DOUBLE> eo_clover_view<PREC_DOUBLE>(lmb_ctx *ctx, int inverse) {
+  return {(const double2 *)eo_buffer(ctx, inverse ? "eo_Ai_d" : "eo_A_d"), ctx->g.V, 1.f};
+}
+template <> Clover<PREC_SINGLE> eo_clover_view<PREC_SINGLE>(lmb_ctx *ctx, int inverse) {
+  return {(const float4 *)eo_buffer(ctx, inverse ? "eo_Ai_s" : "eo_A_s"), ctx->g.V, 1.f};
+}
+template <> Clover<PREC_HALF> eo_clover_view<PREC_HALF>(lmb_ctx *ctx, int inverse) {
+  Clover<PREC_HALF> c;
+  const char *buf = eo_buffer(ctx, inverse ? "eo_Ai_h" : "eo_A_h");
+  c.data = (const int4 *)buf;
+  c.tail = buf ? (const int2 *)(buf + sizeof(int4) * 8 * ctx->g.V) : nullptr;
+  c.V = ctx->g.V;
+  c.scale = (inverse ? ctx->clover_inv : ctx->clover).scale;
+  return c;
+}
+
 // even/odd Schur operator Dh = A_ee - k^2 H_eo A_oo^-1 H_oe on the V/2 even
 // sites (checkerboard order), as the CG driver sees it: launch(dagger = 0)
 // applies Dh^+ and launch(dagger = 1) applies Dh, so the CG solves
@@ -525,18 +634,21 @@ struct SchurPolicy {
     if (rc) return rc;
     rc = ensure_link_precision(ctx, ctx->links[LMB_LINKS_THIN], prec, st);
     if (rc) return rc;
-    if (!clover) return LMB_OK;
-    rc = ensure_clover(ctx, -kappa * csw, PREC_DOUBLE, st);
-    if (rc) return rc;
-    rc = ensure_clover(ctx, -kappa * csw, prec, st);
-    if (rc) return rc;
-    return ensure_clover_inverse(ctx, prec, st);
+    if (clover) {
+      rc = ensure_clover(ctx, -kappa * csw, PREC_DOUBLE, st);
+      if (rc) return rc;
+      rc = ensure_clover(ctx, -kappa * csw, prec, st);
+      if (rc) return rc;
+      rc = ensure_clover_inverse(ctx, prec, st);
+      if (rc) return rc;
+    }
+    return ensure_eo_copies(ctx, prec, clover, st);
   }
   template <int P, bool CL, int DAG, class G, class Epi>
   void launch_cl(lmb_ctx *ctx, const Field<P, 12> &in, const Field<P, 12> &t, const G &U, const Epi &epi,
                  cudaStream_t st) const {
     typedef typename Real<P>::type R;
-    const Clover<P> A = clover_view<P>(ctx->clover, ctx->g.V), Ai = clover_view<P>(ctx->clover_inv, ctx->g.V);
+    const Clover<P> A = eo_clover_view<P>(ctx, 0), Ai = eo_clover_view<P>(ctx, 1);
     const unsigned grid = grid_for(ctx->g.V / 2, kDslashThreads);
     const EpiStoreFollow<P, Epi> e1{t, epi};
     eo_hop_kernel<R, DAG, 0, true, CL><<<grid, kDslashThreads, 0, st>>>(ctx->g, 1, in, in, U, A, Ai, (R)0, (R)1, e1);
@@ -560,9 +672,8 @@ struct SchurPolicy {
   }
   template <int P, class Epi>
   int launch(lmb_ctx *ctx, const Field<P, 12> &in, int dagger, const Epi &epi, cudaStream_t st) const {
-    const LinkSet &ls = ctx->links[LMB_LINKS_THIN];
-    if (ls.recon(P)) return launch_g<P>(ctx, in, gauge12_view<P>(ls, ctx->g.V), dagger, epi, st);
-    return launch_g<P>(ctx, in, gauge_view<P>(ls, ctx->g.V), dagger, epi, st);
+    if (ctx->links[LMB_LINKS_THIN].recon(P)) return launch_g<P>(ctx, in, eo_gauge12_view<P>(ctx), dagger, epi, st);
+    return launch_g<P>(ctx, in, eo_gauge_view<P>(ctx), dagger, epi, st);
   }
   int link_reals(const lmb_ctx *ctx, int prec) const { return ctx->links[LMB_LINKS_THIN].recon(prec) ? 12 : 18; }
 };
@@ -590,8 +701,7 @@ template <bool CL, class G>
 int evenodd_setup_g(lmb_ctx *ctx, const G &U, double kappa, const Field<PREC_DOUBLE, 12> &be,
                     const Field<PREC_DOUBLE, 12> &bo, Field<PREC_DOUBLE, 12> &tb, Field<PREC_DOUBLE, 12> &bh,
                     cudaStream_t st) {
-  const Clover<PREC_DOUBLE> A = clover_view<PREC_DOUBLE>(ctx->clover, ctx->g.V);
-  const Clover<PREC_DOUBLE> Ai = clover_view<PREC_DOUBLE>(ctx->clover_inv, ctx->g.V);
+  const Clover<PREC_DOUBLE> A = eo_clover_view<PREC_DOUBLE>(ctx, 0), Ai = eo_clover_view<PREC_DOUBLE>(ctx, 1);
   const int64_t Vh = ctx->g.V / 2;
   eo_local_kernel<CL><<<grid_for(Vh, 256), 256, 0, st>>>(tb, bo, ctx->g, 1, Ai);  // A_oo^-1 b_o
   EpiStore<PREC_DOUBLE, 12> e{bh, nullptr};
@@ -603,8 +713,7 @@ int evenodd_setup_g(lmb_ctx *ctx, const G &U, double kappa, const Field<PREC_DOU
 template <bool CL, class G>
 int evenodd_odd_g(lmb_ctx *ctx, const G &U, double kappa, const Field<PREC_DOUBLE, 12> &xe,
                   const Field<PREC_DOUBLE, 12> &bo, Field<PREC_DOUBLE, 12> &xo, cudaStream_t st) {
-  const Clover<PREC_DOUBLE> A = clover_view<PREC_DOUBLE>(ctx->clover, ctx->g.V);
-  const Clover<PREC_DOUBLE> Ai = clover_view<PREC_DOUBLE>(ctx->clover_inv, ctx->g.V);
+  const Clover<PREC_DOUBLE> A = eo_clover_view<PREC_DOUBLE>(ctx, 0), Ai = eo_clover_view<PREC_DOUBLE>(ctx, 1);
   EpiStore<PREC_DOUBLE, 12> e{xo, nullptr};
   eo_hop_kernel<double, 0, 1, true, CL><<<grid_for(ctx->g.V / 2, kDslashThreads), kDslashThreads, 0, st>>>(
       ctx->g, 1, xe, bo, U, A, Ai, 1.0, kappa, e);  // x_o = A_oo^-1 (b_o + k H_oe x_e)
@@ -2135,14 +2244,13 @@ int lmb_solve_evenodd(lmb_ctx *ctx, const lmb_cg_params *prm, void *x, const voi
   LMB_CUDA(ctx, cudaStreamSynchronize(st));
   const double bnorm = std::sqrt(bb);
   const double tol = std::max(prm->atol, prm->rtol * bnorm);
-  const LinkSet &ls = ctx->links[LMB_LINKS_THIN];
-  const bool r12 = ls.recon(PREC_DOUBLE);
+  const bool r12 = ctx->links[LMB_LINKS_THIN].recon(PREC_DOUBLE);
   if (clover)
-    rc = r12 ? evenodd_setup_g<true>(ctx, gauge12_view<PREC_DOUBLE>(ls, V), prm->kappa, be, bo, tb, bh, st)
-             : evenodd_setup_g<true>(ctx, gauge_view<PREC_DOUBLE>(ls, V), prm->kappa, be, bo, tb, bh, st);
+    rc = r12 ? evenodd_setup_g<true>(ctx, eo_gauge12_view<PREC_DOUBLE>(ctx), prm->kappa, be, bo, tb, bh, st)
+             : evenodd_setup_g<true>(ctx, eo_gauge_view<PREC_DOUBLE>(ctx), prm->kappa, be, bo, tb, bh, st);
   else
-    rc = r12 ? evenodd_setup_g<false>(ctx, gauge12_view<PREC_DOUBLE>(ls, V), prm->kappa, be, bo, tb, bh, st)
-             : evenodd_setup_g<false>(ctx, gauge_view<PREC_DOUBLE>(ls, V), prm->kappa, be, bo, tb, bh, st);
+    rc = r12 ? evenodd_setup_g<false>(ctx, eo_gauge12_view<PREC_DOUBLE>(ctx), prm->kappa, be, bo, tb, bh, st)
+             : evenodd_setup_g<false>(ctx, eo_gauge_view<PREC_DOUBLE>(ctx), prm->kappa, be, bo, tb, bh, st);
   if (rc) return rc;
   // CGNE on the Schur system; its residual is the full system's, so the
   // stopping rule is |b - D x| <= max(atol, rtol |b|)
@@ -2159,11 +2267,11 @@ int lmb_solve_evenodd(lmb_ctx *ctx, const lmb_cg_params *prm, void *x, const voi
     if (rc) return rc;
   }
   if (clover)
-    rc = r12 ? evenodd_odd_g<true>(ctx, gauge12_view<PREC_DOUBLE>(ls, V), prm->kappa, xe, bo, xo, st)
-             : evenodd_odd_g<true>(ctx, gauge_view<PREC_DOUBLE>(ls, V), prm->kappa, xe, bo, xo, st);
+    rc = r12 ? evenodd_odd_g<true>(ctx, eo_gauge12_view<PREC_DOUBLE>(ctx), prm->kappa, xe, bo, xo, st)
+             : evenodd_odd_g<true>(ctx, eo_gauge_view<PREC_DOUBLE>(ctx), prm->kappa, xe, bo, xo, st);
   else
-    rc = r12 ? evenodd_odd_g<false>(ctx, gauge12_view<PREC_DOUBLE>(ls, V), prm->kappa, xe, bo, xo, st)
-             : evenodd_odd_g<false>(ctx, gauge_view<PREC_DOUBLE>(ls, V), prm->kappa, xe, bo, xo, st);
+    rc = r12 ? evenodd_odd_g<false>(ctx, eo_gauge12_view<PREC_DOUBLE>(ctx), prm->kappa, xe, bo, xo, st)
+             : evenodd_odd_g<false>(ctx, eo_gauge_view<PREC_DOUBLE>(ctx), prm->kappa, xe, bo, xo, st);
   if (rc) return rc;
   if (ctx->dtype == LMB_DTYPE_C128)
     eo_unpack_kernel<double2><<<pgrid, 256, 0, st>>>((double2 *)x, xe, xo, ctx->g, ctx->pd);

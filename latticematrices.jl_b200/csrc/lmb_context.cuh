@@ -102,6 +102,14 @@ struct lmb_ctx {
   bool dw_two_pass = false;
   lmb::CloverCache clover;
   lmb::CloverCache clover_inv;  // A^-1 blocks (even/odd solve)
+  // parity-ordered copies of link / clover storage for the even/odd solve:
+  // workspace name -> (source version, volume, buffer) they were built for
+  struct EoTag {
+    uint64_t version;
+    int64_t V;
+    void *ptr;
+  };
+  std::map<std::string, EoTag> eo_tags;
   std::map<std::string, std::pair<void *, size_t>> buffers;
   double *partials = nullptr;
   size_t partials_cap = 0;

@@ -13,6 +13,10 @@
 // Dh is solved by CG on Dh Dh^+ y = bh_e, x_e = Dh^+ y (CGNE: its residual
 // is bh_e - Dh x_e itself), with Dh^+ = A_ee - k^2 H^+_eo A_oo^-1 H^+_oe.
 //
+// Links and clover blocks are read from parity-ordered copies (site s at
+// parity(s) V/2 + s/2, every plane permuted alike), so the sites of one
+// parity are contiguous and no sector carries the other parity's data.
+//
 // Parity: a site is even when its global coordinate sum is
 // (_global_site_is_even, LatticeMatrices.jl:357-363; the even/odd kernels
 // of linearalgebra_D.jl:2815-2930 use the same rule).  Half fields hold the
@@ -34,6 +38,18 @@ LMB_D int cb_site(const Geom &g, int cb, int p, int c[4]) {
   const int fix = (coord_parity(g, c) + p) & 1;
   c[0] += fix;
   return lex0 + fix;
+}
+
+// site s at parity(s) V/2 + s/2 in each of `nplanes` planes of V elements
+template <typename T>
+__global__ void __launch_bounds__(256)
+    eo_permute_kernel(T *dst, const T *src, int nplanes, const Geom g) {
+  const int64_t s = (int64_t)blockIdx.x * 256 + threadIdx.x;
+  if (s >= g.V) return;
+  int c[4];
+  site_coords(g, (int)s, c);
+  const int64_t e = (int64_t)coord_parity(g, c) * (g.V / 2) + (s >> 1);
+  for (int k = 0; k < nplanes; k++) dst[k * g.V + e] = src[k * g.V + s];
 }
 
 // ---------------------------------------------------------------------------
@@ -151,36 +167,37 @@ __global__ void __launch_bounds__(128) clover_invert_kernel(double2 *dst, const 
 // ---------------------------------------------------------------------------
 // half-field kernels
 // ---------------------------------------------------------------------------
-// hop of direction MU into site s (lexicographic) from the opposite-parity
-// half field `in` (neighbour n at checkerboard index n / 2)
+// hop of direction MU into site s (lexicographic, parity p, parity-ordered
+// index es) from the opposite-parity half field `in` (neighbour n at
+// checkerboard index n / 2); U parity-ordered
 template <typename R, int DAG, int MU, class SF, class G>
-LMB_D void eo_hop(const Geom &g, int s, const int *c, const SF &in, const G &U, Cx<R> *acc) {
+LMB_D void eo_hop(const Geom &g, int s, int64_t es, int p, const int *c, const SF &in, const G &U, Cx<R> *acc) {
   constexpr int FPM = DAG ? +1 : -1;
   constexpr int BPM = -FPM;
-  Cx<R> p[12], h[6], uh[6], u[9];
+  Cx<R> q[12], h[6], uh[6], u[9];
   int wrap;
   {
     const int sp = fwd_site(g, s, c, MU, 1, &wrap);
-    in.load(sp >> 1, p);
-    project<FPM, MU>(p, h);
+    in.load(sp >> 1, q);
+    project<FPM, MU>(q, h);
     if (wrap && ((g.phase_mask >> MU) & 1)) scale_phase(h, 6, g.ph_fwd[MU]);
-    U.load(MU, s, u);
+    U.load(MU, es, u);
     su3_mul_half(u, h, uh);
     reconstruct<FPM, MU>(acc, uh);
   }
   {
     const int sm = bwd_site(g, s, c, MU, 1, &wrap);
-    in.load(sm >> 1, p);
-    project<BPM, MU>(p, h);
+    in.load(sm >> 1, q);
+    project<BPM, MU>(q, h);
     if (wrap && ((g.phase_mask >> MU) & 1)) scale_phase(h, 6, g.ph_bwd[MU]);
-    U.load(MU, sm, u);
+    U.load(MU, (int64_t)(1 - p) * (g.V / 2) + (sm >> 1), u);
     su3_adj_mul_half(u, h, uh);
     reconstruct<BPM, MU>(acc, uh);
   }
 }
 
 template <typename R, class C>
-LMB_D void clover_apply(const C &A, int s, Cx<R> *v) {
+LMB_D void clover_apply(const C &A, int64_t s, Cx<R> *v) {
 #pragma unroll
   for (int blk = 0; blk < 2; blk++) {
     R a[36];
@@ -192,7 +209,8 @@ LMB_D void clover_apply(const C &A, int s, Cx<R> *v) {
   }
 }
 
-// Sites of parity p (one thread per checkerboard index):
+// Sites of parity p (one thread per checkerboard index; links and clover
+// blocks parity-ordered):
 //   v = c1 W(x) [WMODE 1]  or  c1 A(x) W(x) [WMODE 2]  (W: parity p)
 //     + c2 (H in)(x)        (H^+ when DAG; in: parity 1 - p)
 //   out = A^-1(x) v when AINV, else v.     CL = false: A = 1.
@@ -207,28 +225,30 @@ __global__ void __launch_bounds__(kDslashThreads)
   if (active) {
     int c[4];
     const int s = cb_site(g, (int)cb, p, c);
+    const int64_t es = (int64_t)p * (g.V / 2) + cb;
     Cx<R> acc[12];
 #pragma unroll
     for (int k = 0; k < 12; k++) acc[k] = Cx<R>(0, 0);
-    eo_hop<R, DAG, 0>(g, s, c, in, U, acc);
-    eo_hop<R, DAG, 1>(g, s, c, in, U, acc);
-    eo_hop<R, DAG, 2>(g, s, c, in, U, acc);
-    eo_hop<R, DAG, 3>(g, s, c, in, U, acc);
+    eo_hop<R, DAG, 0>(g, s, es, p, c, in, U, acc);
+    eo_hop<R, DAG, 1>(g, s, es, p, c, in, U, acc);
+    eo_hop<R, DAG, 2>(g, s, es, p, c, in, U, acc);
+    eo_hop<R, DAG, 3>(g, s, es, p, c, in, U, acc);
 #pragma unroll
     for (int k = 0; k < 12; k++) v[k] = c2 * acc[k];
     if constexpr (WMODE != 0) {
       Cx<R> w[12];
       W.load(cb, w);
-      if constexpr (WMODE == 2 && CL) clover_apply<R>(A, s, w);
+      if constexpr (WMODE == 2 && CL) clover_apply<R>(A, es, w);
 #pragma unroll
       for (int k = 0; k < 12; k++) v[k] = v[k] + c1 * w[k];
     }
-    if constexpr (AINV && CL) clover_apply<R>(Ainv, s, v);
+    if constexpr (AINV && CL) clover_apply<R>(Ainv, es, v);
   }
   epi((int)(active ? cb : 0), active, v);
 }
 
-// out = A^-1 in on the sites of parity p (CL = false: a copy)
+// out = A^-1 in on the sites of parity p (CL = false: a copy; Ainv
+// parity-ordered)
 template <bool CL, class C>
 __global__ void __launch_bounds__(256)
     eo_local_kernel(Field<PREC_DOUBLE, 12> out, const Field<PREC_DOUBLE, 12> in, const Geom g, const int p,
@@ -237,11 +257,7 @@ __global__ void __launch_bounds__(256)
   if (cb >= g.V / 2) return;
   Cx<double> v[12];
   in.load(cb, v);
-  if constexpr (CL) {
-    int c[4];
-    const int s = cb_site(g, (int)cb, p, c);
-    clover_apply<double>(Ainv, s, v);
-  }
+  if constexpr (CL) clover_apply<double>(Ainv, (int64_t)p * (g.V / 2) + cb, v);
   out.store(cb, v);
 }
 
