@@ -243,6 +243,19 @@ int lmb_wilson_clover_fermion_force(lmb_ctx *ctx, const void *const U[4],
  * 392-399). */
 int lmb_clover_field_strength(lmb_ctx *ctx, void *const F[6], void *stream);
 
+/* set_halo! (LatticeMatrices_core.jl:550-567) of a single-rank padded field
+ * (exchange_dim_local!, :707-723): the nw-deep ghost layer of every one of
+ * the D (4 or 5) dimensions is filled from the periodic image of the core,
+ * times phase_d on the plus side and 1/phase_d on the minus side, corners
+ * with the product of the phases they wrap in -- the values the reference's
+ * dimension-by-dimension exchange leaves.  field: (ncomp complex, L_1+2nw,
+ * ..., L_D+2nw) column-major, dtype LMB_DTYPE_C128 or LMB_DTYPE_C64; the core
+ * is read, only ghosts are written.  Needs no context (no state); returns
+ * LMB_ERR_ARG for bad sizes, nw > L_d or a zero phase.  Stream-ordered. */
+int lmb_set_halo(void *field, int dtype, int ncomp, int D, const int *L,
+                 int nw, const double *phase_re, const double *phase_im,
+                 void *stream);
+
 /* Solve D x = b for the Wilson or Wilson-clover operator (params->op,
  * kappa, csw) by even/odd (Schur) preconditioning: the even half lattice
  * carries Dh = A_ee - kappa^2 H_eo A_oo^-1 H_oe, solved by CG on Dh Dh^+

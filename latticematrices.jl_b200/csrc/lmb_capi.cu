@@ -14,6 +14,7 @@
 #include "lmb_clover_force.cuh"
 #include "lmb_domainwall.cuh"
 #include "lmb_evenodd.cuh"
+#include "lmb_halo.cuh"
 
 using namespace lmb;
 
@@ -2302,6 +2303,37 @@ int lmb_solve_evenodd(lmb_ctx *ctx, const lmb_cg_params *prm, void *x, const voi
   if (!res->converged && res->reason == LMB_CG_CONVERGED) res->reason = LMB_CG_MAXIMUM_ITERATIONS;
   res->kernel_launches += 11;
   return LMB_OK;
+}
+
+int lmb_set_halo(void *field, int dtype, int ncomp, int D, const int *L, int nw, const double *phase_re,
+                 const double *phase_im, void *stream) {
+  if (!field || !L || !phase_re || !phase_im) return LMB_ERR_ARG;
+  if ((dtype != LMB_DTYPE_C128 && dtype != LMB_DTYPE_C64) || ncomp <= 0 || (D != 4 && D != 5) || nw < 0)
+    return LMB_ERR_ARG;
+  HaloGeom h{};
+  h.D = D;
+  h.nw = nw;
+  h.npad = 1;
+  for (int d = 0; d < D; d++) {
+    if (L[d] <= 0 || nw > L[d]) return LMB_ERR_ARG;
+    const double re = phase_re[d], im = phase_im[d], m2 = re * re + im * im;
+    if (!(m2 > 0) || !std::isfinite(m2)) return LMB_ERR_ARG;
+    h.L[d] = L[d];
+    h.P[d] = L[d] + 2 * nw;
+    h.ph[d][0] = re;
+    h.ph[d][1] = im;
+    h.iph[d][0] = re / m2;
+    h.iph[d][1] = -im / m2;
+    h.npad *= h.P[d];
+  }
+  if (nw == 0) return LMB_OK;
+  cudaStream_t st = as_stream(stream);
+  const unsigned grid = grid_for(h.npad, 256);
+  if (dtype == LMB_DTYPE_C128)
+    set_halo_kernel<double2><<<grid, 256, 0, st>>>((double2 *)field, ncomp, h);
+  else
+    set_halo_kernel<float2><<<grid, 256, 0, st>>>((float2 *)field, ncomp, h);
+  return cudaGetLastError() == cudaSuccess ? LMB_OK : LMB_ERR_CUDA;
 }
 
 int lmb_domainwall_set(lmb_ctx *ctx, int L5, double mass, double M, const double *a, const double *b,

@@ -6,8 +6,9 @@ include/lmb200.h).  Julia names map as `mul!` -> `mul_`, `cg!` -> `cg_`,
 `adjoint(D)`.
 """
 from ._lib import ArgumentError, DimensionMismatch, LMBError, load, EXPORTED, LIB_PATH  # noqa: F401
-from .lattice import (LatticeMatrix, clear_matrix_, halo_is_dirty,  # noqa: F401
-                      mark_halo_dirty_, similar, substitute_)
+from .lattice import (LatticeMatrix, clear_matrix_, ensure_halo_,  # noqa: F401
+                      halo_is_dirty, mark_halo_dirty_, set_halo_, similar,
+                      substitute_)
 from .operators import (CloverFieldStrength4D, WilsonDiracCloverOperator4D,  # noqa: F401
                         WilsonDiracOperator4D, adjoint, mul_,
                         StaggeredDiracOperator4D, HISQLinks4D,

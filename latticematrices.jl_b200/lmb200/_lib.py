@@ -39,6 +39,7 @@ EXPORTED = (
     "lmb_hisq_link_pullback", "lmb_hisq_fermion_force",
     "lmb_wilson_clover_link_pullback", "lmb_wilson_clover_fermion_force",
     "lmb_domainwall_set", "lmb_domainwall_apply", "lmb_solve_evenodd",
+    "lmb_set_halo",
 )
 
 
@@ -169,6 +170,9 @@ def load(path: str = LIB_PATH):
             pvp, vp]
         lib.lmb_cg_ddagd.argtypes = [vp, ctypes.POINTER(CGParams), vp, vp,
                                      ctypes.POINTER(CGResultC), vp]
+        lib.lmb_set_halo.argtypes = [vp, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_int, ip, ctypes.c_int, dp, dp,
+                                     vp]
         lib.lmb_solve_evenodd.argtypes = [vp, ctypes.POINTER(CGParams), vp,
                                           vp, ctypes.POINTER(CGResultC), vp]
         lib.lmb_field_dot.argtypes = [vp, vp, vp, ctypes.c_int, dp, vp]

@@ -10,16 +10,17 @@ its data pointer is what the C ABI receives.  A 5D field (domain-wall
 fermions, DiracOperators_5D.jl) adds the fifth coordinate s as the slowest
 index: (NC1, NC2, X+2nw, .., T+2nw, L5+2nw).
 
-Single-rank only (PEs = (1,1,1,1)): the halo is never filled, because the
-kernels wrap periodically with the fermion phase; `halo_epoch` still tracks
-core writes so that link caches can be invalidated exactly as
-mark_halo_dirty! does (LatticeMatrices_core.jl:196-203).
+Single-rank only (PEs = (1,1,1,1)).  The stencil kernels wrap periodically
+with the fermion phase and never read the halo; set_halo_ / ensure_halo_
+fill it on request (lmb_set_halo).  `halo_epoch` tracks core writes so that
+link caches are invalidated and ensure_halo_ refills exactly as
+mark_halo_dirty! / ensure_halo! do (LatticeMatrices_core.jl:196-203, 569-581).
 """
 from __future__ import annotations
 
 import numpy as np
 
-from ._lib import ArgumentError
+from ._lib import ArgumentError, LMBError
 
 _DTYPES = {np.dtype(np.complex128): 0, np.dtype(np.complex64): 1}
 
@@ -152,6 +153,41 @@ def mark_halo_dirty_(ls: LatticeMatrix):
 
 def halo_is_dirty(ls: LatticeMatrix) -> bool:
     return ls.halo_epoch.core != ls.halo_epoch.halo
+
+
+def set_halo_(ls: LatticeMatrix):
+    """set_halo!(ls) (LatticeMatrices_core.jl:550-567) on one process: the
+    ghosts take the periodic image of the core times the boundary phase
+    (exchange_dim_local!, :707-723), written by liblmb200's lmb_set_halo on
+    the field's device; the halo epoch is then clean."""
+    if ls.nw > 0:
+        import ctypes
+        import torch
+        from ._lib import load
+        if ls.A.device.type != "cuda":
+            raise LMBError("set_halo! runs in liblmb200 on the GPU; the field is on "
+                           f"{ls.A.device}")
+        lib = load()
+        D = ls.dim
+        L = (ctypes.c_int * D)(*ls.gsize)
+        re = (ctypes.c_double * D)(*[complex(p).real for p in ls.phases])
+        im = (ctypes.c_double * D)(*[complex(p).imag for p in ls.phases])
+        with torch.cuda.device(ls.A.device):
+            st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+            rc = lib.lmb_set_halo(ls.A.data_ptr(), ls.dtype_code,
+                                  ls.NC1 * ls.NC2, D, L, ls.nw, re, im, st)
+        if rc == -1:
+            raise ArgumentError("lmb_set_halo rejected the field geometry")
+        if rc != 0:
+            raise LMBError(f"lmb_set_halo failed ({rc})")
+    ls.halo_epoch.halo = ls.halo_epoch.core
+
+
+def ensure_halo_(ls: LatticeMatrix):
+    """ensure_halo!(ls) (LatticeMatrices_core.jl:569-581): set_halo! only
+    when the core changed since the last fill."""
+    if halo_is_dirty(ls):
+        set_halo_(ls)
 
 
 def similar(ls: LatticeMatrix) -> LatticeMatrix:

@@ -457,3 +457,24 @@ def domainwall_dense(links, psi, mass, M, a, b, c, phases, adjoint=False):
         return q - Fq + B * Dq + domainwall_F_dense(C * Dq, mass, adjoint=True)
     Fpsi = domainwall_F_dense(psi, mass)
     return A * (psi - Fpsi + domainwall_DW_dense(links, B * psi + C * Fpsi, M, phases))
+
+
+# ---------------------------------------------------------------------------
+# halo fill (LatticeMatrices_core.jl:550-567, 707-723)
+# ---------------------------------------------------------------------------
+def set_halo_dense(A, nw, phases):
+    """set_halo! on one process, dimension by dimension as
+    exchange_dim_local! does: the minus ghost slab takes the plus face divided
+    by phase_d, the plus ghost slab the minus face times phase_d; slabs span
+    the full padded extent of the other dimensions.  A: padded array in the
+    reference's order (NC1, NC2, X+2nw, ...)."""
+    A = np.array(A, copy=True)
+    for d in range(A.ndim - 2):
+        ax = d + 2
+        n = A.shape[ax]
+
+        def sl(r):
+            return tuple(r if i == ax else slice(None) for i in range(A.ndim))
+        A[sl(slice(0, nw))] = A[sl(slice(n - 2 * nw, n - nw))] / phases[d]
+        A[sl(slice(n - nw, n))] = A[sl(slice(nw, 2 * nw))] * phases[d]
+    return A

@@ -141,3 +141,17 @@ def test_domainwall_validation_before_cuda():
         lmb.mul_(other.similar(), D, other)
     with pytest.raises(lmb.ArgumentError, match="distinct|alias"):
         lmb.cg_(psi, lmb.DdagDOp(D, out), psi)
+
+
+def test_halo_fill_host_rules():
+    """nw = 0 has no ghosts (set_halo! only marks the epoch clean); a field
+    off the GPU cannot be filled (the fill is the library's kernel)."""
+    import lmb200 as lmb
+    flat = _cpu_field(lmb, 3, 4, nw=0)
+    lmb.mark_halo_dirty_(flat)
+    lmb.set_halo_(flat)
+    assert not lmb.halo_is_dirty(flat)
+    f = _cpu_field(lmb, 3, 4)
+    lmb.mark_halo_dirty_(f)
+    with pytest.raises(lmb.LMBError, match="GPU"):
+        lmb.ensure_halo_(f)
