@@ -7,7 +7,7 @@ import ctypes
 import numpy as np
 
 from ._lib import ArgumentError
-from .lattice import mark_halo_dirty_
+from .lattice import require_single_rank, mark_halo_dirty_
 from .operators import WilsonDiracCloverOperator4D, _stream
 
 
@@ -56,6 +56,7 @@ def wilson_clover_link_pullback_(dlinks, cache, links, result_cotangent, psi, co
     _validate(dlinks, cache, links, result_cotangent, psi)
     st = _stream()
     ctx = cache.ctx
+    require_single_rank(psi)
     ctx.set_geometry(psi.gsize, psi.nw, psi.phases, psi.coords, psi.dtype_code)
     ctx.check(ctx.lib.lmb_wilson_clover_link_pullback(
         ctx.handle, _ptrs(links), cache.kappa, cache.cSW, float(coefficient),
@@ -80,6 +81,7 @@ def wilson_clover_fermion_force_(dlinks, D, phi, *, rtol=1e-12, atol=0.0, maxite
     res = CGResultC()
     st = _stream()
     ctx = D.ctx
+    require_single_rank(phi)
     ctx.set_geometry(phi.gsize, phi.nw, phi.phases, phi.coords, phi.dtype_code)
     ep = (ctypes.c_uint64 * 4)(*[u.halo_epoch.core for u in D.U])
     ctx.check(ctx.lib.lmb_wilson_clover_fermion_force(

@@ -25,7 +25,7 @@ import math
 import numpy as np
 
 from ._lib import ArgumentError, DimensionMismatch, PREC
-from .lattice import mark_halo_dirty_
+from .lattice import require_single_rank, mark_halo_dirty_
 from .operators import _Adjoint, _LinkOperator, _stream, _NC_SUPPORTED
 
 
@@ -55,6 +55,7 @@ class _DomainwallBase(_LinkOperator):
         return self._abc
 
     def _bind(self, psi, stream):
+        require_single_rank(psi)
         ctx = self.ctx
         ctx.set_geometry(psi.gsize[:4], psi.nw, psi.phases[:4],
                          psi.coords[:4], psi.dtype_code)
@@ -73,6 +74,7 @@ class _DomainwallBase(_LinkOperator):
         return ctx
 
     def _validate(self, out, psi):
+        require_single_rank(psi)
         if out is psi:
             raise ArgumentError("mul! requires distinct result and input fields")
         for f, what in ((out, "result"), (psi, "fermion")):

@@ -10,7 +10,7 @@ import ctypes
 import numpy as np
 
 from ._lib import ArgumentError, Context
-from .lattice import mark_halo_dirty_
+from .lattice import require_single_rank, mark_halo_dirty_
 from .operators import (HISQDiracOperator4D, HISQLinks4D, _AdjointApply,
                         _stream, _validate_staggered_application,
                         _validate_staggered_links)
@@ -30,6 +30,7 @@ def _ctx_for(field):
     if dev not in _CTX:
         _CTX[dev] = Context(dev)
     c = _CTX[dev]
+    require_single_rank(field)
     c.set_geometry(field.gsize, field.nw, (1, 1, 1, 1), field.coords,
                    field.dtype_code)
     return c
@@ -157,6 +158,7 @@ class HISQDiracCache4D:
         return self
 
     def _bind(self, psi, stream):
+        require_single_rank(psi)
         ctx = self.ctx
         ctx.set_geometry(psi.gsize, psi.nw, psi.phases, psi.coords,
                          psi.dtype_code)
@@ -230,6 +232,7 @@ def hisq_link_pullback_(dthin_links, cache, thin_links, result_cotangent, psi,
     cache.update_(thin_links)
     st = _stream()
     ctx = cache.ctx
+    require_single_rank(psi)
     ctx.set_geometry(psi.gsize, psi.nw, psi.phases, psi.coords, psi.dtype_code)
     ctx.check(ctx.lib.lmb_hisq_link_pullback(
         ctx.handle, _ptrs(thin_links), cache.naik_epsilon, float(coefficient),
@@ -255,6 +258,7 @@ def hisq_fermion_force_(dthin_links, cache, phi, *, rtol=1e-12, atol=0.0,
     res = CGResultC()
     st = _stream()
     ctx = cache.ctx
+    require_single_rank(phi)
     ctx.set_geometry(phi.gsize, phi.nw, phi.phases, phi.coords, phi.dtype_code)
     ep = (ctypes.c_uint64 * 4)(*[u.halo_epoch.core for u in thin])
     ctx.check(ctx.lib.lmb_hisq_fermion_force(

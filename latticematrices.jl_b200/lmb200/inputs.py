@@ -10,7 +10,7 @@ import ctypes
 import numpy as np
 
 from ._lib import ArgumentError, Context
-from .lattice import LatticeMatrix, mark_halo_dirty_
+from .lattice import require_single_rank, LatticeMatrix, mark_halo_dirty_
 from .operators import _stream
 
 _CTX = {}
@@ -21,6 +21,7 @@ def _ctx(field: LatticeMatrix) -> Context:
     if dev not in _CTX:
         _CTX[dev] = Context(dev)
     c = _CTX[dev]
+    require_single_rank(field)
     c.set_geometry(field.gsize, field.nw, field.phases, field.coords,
                    field.dtype_code)
     return c

@@ -10,9 +10,14 @@ its data pointer is what the C ABI receives.  A 5D field (domain-wall
 fermions, DiracOperators_5D.jl) adds the fifth coordinate s as the slowest
 index: (NC1, NC2, X+2nw, .., T+2nw, L5+2nw).
 
-Single-rank only (PEs = (1,1,1,1)).  The stencil kernels wrap periodically
-with the fermion phase and never read the halo; set_halo_ / ensure_halo_
-fill it on request (lmb_set_halo).  `halo_epoch` tracks core writes so that
+One rank per lattice for the stencils (PEs = (1,1,1,1)): they wrap
+periodically with the fermion phase and never read the halo; set_halo_ /
+ensure_halo_ fill it on request (lmb_set_halo).  A process grid PEs with
+prod(PEs) ranks of an initialised torch.distributed group (NCCL, or gloo on
+CPU) splits the lattice into blocks of PN = gsize / PEs sites (rank r at the
+row-major Cartesian coordinates of r, as MPI_Cart_create numbers them); such
+fields support the halo exchange (exchange_dim!, distributed.py), gather and
+dot, not the stencils.  `halo_epoch` tracks core writes so that
 link caches are invalidated and ensure_halo_ refills exactly as
 mark_halo_dirty! / ensure_halo! do (LatticeMatrices_core.jl:196-203, 569-581).
 """
@@ -66,13 +71,16 @@ class LatticeMatrix:
         if any(p == 0 for p in phases):
             raise ArgumentError(
                 "boundary phases must be nonzero because negative wraps use inv(phase)")
-        if tuple(PEs) != (1,) * dim:
-            raise ArgumentError(
-                "one process per GPU: this build takes a single-rank process grid")
+        PEs = tuple(int(v) for v in PEs)
+        coords = (0,) * dim
+        if PEs != (1,) * dim:
+            from .distributed import cart_coords
+            coords = cart_coords(PEs, gsize)
+        PN = tuple(g // p for g, p in zip(gsize, PEs))
         for d in range(dim):
-            if nw > gsize[d]:
+            if nw > PN[d]:
                 raise ArgumentError(
-                    f"halo width nw={nw} exceeds local lattice size {gsize[d]} "
+                    f"halo width nw={nw} exceeds local lattice size {PN[d]} "
                     f"in dimension {d + 1}; the nearest-neighbor halo exchange "
                     f"requires nw <= local size")
         dt = np.dtype(elementtype)
@@ -81,14 +89,14 @@ class LatticeMatrix:
         import torch
         self.NC1, self.NC2, self.dim = int(NC1), int(NC2), dim
         self.gsize = gsize
-        self.PN = gsize
+        self.PN = PN
         self.nw = int(nw)
         self.phases = tuple(phases)
         self.elementtype = dt
-        self.coords = (0,) * dim
-        self.dims = (1,) * dim
+        self.coords = coords
+        self.dims = PEs
         self.halo_epoch = HaloEpoch()
-        padded = tuple(v + 2 * self.nw for v in gsize)
+        padded = tuple(v + 2 * self.nw for v in PN)
         tdt = torch.complex128 if dt == np.complex128 else torch.complex64
         self.A = torch.zeros(padded[::-1] + (self.NC2, self.NC1), dtype=tdt,
                              device=device)
@@ -103,7 +111,9 @@ class LatticeMatrix:
             PEs = (1,) * dim
         lm = cls(NC1, NC2, dim, A.shape[2:], PEs, nw=nw,
                  elementtype=A.dtype, phases=phases, device=device)
-        lm.set_core(A)
+        # every rank keeps its block of the global array
+        block = tuple(slice(c * n, (c + 1) * n) for c, n in zip(lm.coords, lm.PN))
+        lm.set_core(A[(slice(None), slice(None)) + block])
         return lm
 
     @property
@@ -115,23 +125,29 @@ class LatticeMatrix:
 
     def core_view(self):
         n = self.nw
-        return self.A[tuple(slice(n, n + v) for v in self.gsize[::-1])]
+        return self.A[tuple(slice(n, n + v) for v in self.PN[::-1])]
 
     def set_core(self, A):
         import torch
         A = np.asarray(A, dtype=self.elementtype)
-        if A.shape != (self.NC1, self.NC2) + self.gsize:
+        if A.shape != (self.NC1, self.NC2) + self.PN:
             raise ArgumentError(
-                f"array shape {A.shape} does not match lattice "
-                f"{(self.NC1, self.NC2) + self.gsize}")
+                f"array shape {A.shape} does not match the local lattice "
+                f"{(self.NC1, self.NC2) + self.PN}")
         host = torch.from_numpy(np.ascontiguousarray(A.T))
         self.core_view().copy_(host.to(self.A.device))
         mark_halo_dirty_(self)
 
     def gather_matrix(self):
-        """Core values as a Fortran-ordered (NC1, NC2, X, Y, Z, T[, L5]) array
-        (gather_matrix, LatticeMatrices_core.jl:936-993)."""
-        return np.asfortranarray(self.core_view().cpu().numpy().T)
+        """Core values of the whole lattice as a Fortran-ordered
+        (NC1, NC2, X, Y, Z, T[, L5]) array (gather_matrix,
+        LatticeMatrices_core.jl:936-993); every rank of a process grid gets
+        the assembled array."""
+        local = np.asfortranarray(self.core_view().cpu().numpy().T)
+        if self.dims == (1,) * self.dim:
+            return local
+        from .distributed import gather_blocks
+        return gather_blocks(self, local)
 
     def similar(self):
         return LatticeMatrix(self.NC1, self.NC2, self.dim, self.gsize,
@@ -160,7 +176,10 @@ def set_halo_(ls: LatticeMatrix):
     ghosts take the periodic image of the core times the boundary phase
     (exchange_dim_local!, :707-723), written by liblmb200's lmb_set_halo on
     the field's device; the halo epoch is then clean."""
-    if ls.nw > 0:
+    if ls.nw > 0 and ls.dims != (1,) * ls.dim:
+        from .distributed import exchange_halo
+        exchange_halo(ls)
+    elif ls.nw > 0:
         import ctypes
         import torch
         from ._lib import load
@@ -188,6 +207,15 @@ def ensure_halo_(ls: LatticeMatrix):
     when the core changed since the last fill."""
     if halo_is_dirty(ls):
         set_halo_(ls)
+
+
+def require_single_rank(ls: LatticeMatrix):
+    """The stencils and solvers take one rank per lattice."""
+    if ls.dims != (1,) * ls.dim:
+        raise ArgumentError(
+            f"the sm_100a stencils run one rank per lattice; this field is split "
+            f"over the process grid {ls.dims} (halo exchange, gather and dot "
+            f"support that)")
 
 
 def similar(ls: LatticeMatrix) -> LatticeMatrix:

@@ -14,7 +14,7 @@ import ctypes
 import numpy as np
 
 from ._lib import (ArgumentError, Context, LINKS_THIN, PREC)
-from .lattice import LatticeMatrix, mark_halo_dirty_
+from .lattice import require_single_rank, LatticeMatrix, mark_halo_dirty_
 
 _NC_SUPPORTED = 3
 
@@ -44,6 +44,7 @@ def _validate_links(U, what="gauge link"):
 
 
 def _validate_application(result, U, psi, nc2):
+    require_single_rank(psi)
     if result is psi:
         raise ArgumentError("mul! requires distinct result and input fields")
     if not result.same_geometry(psi):
@@ -97,6 +98,7 @@ class _LinkOperator:
         return self._ctx
 
     def _bind(self, psi, stream):
+        require_single_rank(psi)
         ctx = self.ctx
         ctx.set_geometry(psi.gsize, psi.nw, psi.phases, psi.coords,
                          psi.dtype_code)
@@ -268,6 +270,7 @@ def _validate_staggered_links(U, label="gauge link U"):
 
 
 def _validate_staggered_application(result, links, psi, what="gauge link U"):
+    require_single_rank(psi)
     """_validate_staggered_application (StaggeredDiracOperator.jl:66-92)."""
     if result is psi:
         raise ArgumentError("staggered mul! requires distinct result and input fields")
@@ -387,6 +390,7 @@ class HISQDiracOperator4D:
 
     def _bind(self, psi, stream):
         from ._lib import LINKS_FAT, LINKS_LONG
+        require_single_rank(psi)
         ctx = self.ctx
         ctx.set_geometry(psi.gsize, psi.nw, psi.phases, psi.coords,
                          psi.dtype_code)

@@ -19,7 +19,7 @@ import numpy as np
 from ._lib import (ArgumentError, CG_REASONS, CGParams, CGResultC, PREC,
                    OP_DOMAINWALL, OP_HISQ, OP_STAGGERED, OP_WILSON,
                    OP_WILSON_CLOVER)
-from .lattice import LatticeMatrix, mark_halo_dirty_
+from .lattice import require_single_rank, LatticeMatrix, mark_halo_dirty_
 from .operators import (HISQDiracOperator4D, StaggeredDiracOperator4D,
                         WilsonDiracCloverOperator4D, WilsonDiracOperator4D,
                         _stream, adjoint, mul_)
@@ -115,6 +115,7 @@ def cg_(x, A, b, r=None, p=None, Ap=None, *, rtol=1e-10, atol=0.0,
         raise ArgumentError(f"unknown precision {precision!r}")
     native = _native_operator(A)
     if native is not None:
+        require_single_rank(b)
         D, op = native
         binder = D.wilson if op == OP_WILSON_CLOVER else D
         prm = CGParams()
@@ -266,12 +267,17 @@ def dot(a: LatticeMatrix, b: LatticeMatrix, ctx=None) -> complex:
     if a.elementtype != b.elementtype:
         raise ArgumentError("dot requires fields of the same element type")
     ctx = ctx or _dot_context(a)
-    ctx.set_geometry(a.gsize, a.nw, a.phases, a.coords, a.dtype_code)
+    # the local block (the whole lattice on one rank)
+    ctx.set_geometry(a.PN, a.nw, a.phases, a.coords, a.dtype_code)
     out = (ctypes.c_double * 2)()
     st = _stream()
     ctx.check(ctx.lib.lmb_field_dot(ctx.handle, a.data_ptr(), b.data_ptr(),
                                     a.NC1 * a.NC2, out, st))
-    return complex(out[0], out[1])
+    local = complex(out[0], out[1])
+    if a.dims != (1,) * a.dim:
+        from .distributed import allreduce_complex
+        return allreduce_complex(local, a.A.device)
+    return local
 
 
 _DOT_CTX = {}
