@@ -98,6 +98,8 @@ def exchange_halo(ls):
             send_m.mul_(ph)
         if ls.coords[d] == ls.dims[d] - 1 and ph != 1:
             send_p.mul_(1 / ph)
+        if _host_staged(dist, ls.A):
+            send_m, send_p = send_m.cpu(), send_p.cpu()
         recv_m = torch.empty_like(send_p)
         recv_p = torch.empty_like(send_m)
         # tags as exchange_dim!: a minus face arrives as a plus ghost (tag d),
@@ -109,15 +111,21 @@ def exchange_halo(ls):
                dist.P2POp(dist.irecv, torch.view_as_real(recv_m), rm, tag=d + D)]
         for req in dist.batch_isend_irecv(ops):
             req.wait()
-        gminus.copy_(recv_m)
-        gplus.copy_(recv_p)
+        gminus.copy_(recv_m.to(ls.A.device))
+        gplus.copy_(recv_p.to(ls.A.device))
+
+
+def _host_staged(dist, t):
+    """gloo moves CPU tensors: CUDA data goes through host copies."""
+    return t.is_cuda and dist.get_backend() == "gloo"
 
 
 def gather_blocks(ls, local):
     """The global core assembled from every rank's block (Fortran order)."""
     import torch
     dist = _dist()
-    t = torch.view_as_real(torch.from_numpy(np.ascontiguousarray(local.T)).to(ls.A.device))
+    dev = "cpu" if _host_staged(dist, ls.A) else ls.A.device
+    t = torch.view_as_real(torch.from_numpy(np.ascontiguousarray(local.T)).to(dev))
     parts = [torch.empty_like(t) for _ in range(dist.get_world_size())]
     dist.all_gather(parts, t)
     out = np.zeros((ls.NC1, ls.NC2) + ls.gsize, dtype=ls.elementtype, order="F")
@@ -132,6 +140,8 @@ def allreduce_complex(z, device):
     """Sum of a complex partial result over the ranks (FP64)."""
     import torch
     dist = _dist()
+    if str(device).startswith("cuda") and dist.get_backend() == "gloo":
+        device = "cpu"
     t = torch.tensor([complex(z).real, complex(z).imag], dtype=torch.float64, device=device)
     dist.all_reduce(t)
     return complex(float(t[0]), float(t[1]))

@@ -37,14 +37,23 @@ def _validate_links(U, what="gauge link"):
             raise ArgumentError("all gauge links must have the same global lattice size")
         if link.nw != ref.nw:
             raise ArgumentError("all gauge links must have the same halo width")
+        if link.dims != ref.dims:
+            raise ArgumentError("all gauge links must use the same process grid")
         if any(p != 1 for p in link.phases):
             raise ArgumentError(f"{what} U[{mu}] must use periodic boundary phases")
         if link.elementtype != ref.elementtype:
             raise ArgumentError("all gauge links must have the same element type")
 
 
-def _validate_application(result, U, psi, nc2):
-    require_single_rank(psi)
+def _validate_application(result, U, psi, nc2, split_ok=False):
+    if not split_ok:
+        require_single_rank(psi)
+    elif psi.dims != (1,) * psi.dim:
+        if psi.nw < 1:
+            raise ArgumentError("a field split over a process grid needs nw >= 1 "
+                                "for its neighbours' ghosts")
+        if any(link.dims != psi.dims for link in U):
+            raise ArgumentError("gauge links and fermion field use different process grids")
     if result is psi:
         raise ArgumentError("mul! requires distinct result and input fields")
     if not result.same_geometry(psi):
@@ -98,10 +107,30 @@ class _LinkOperator:
         return self._ctx
 
     def _bind(self, psi, stream):
-        require_single_rank(psi)
+        if psi.dims != (1,) * psi.dim:
+            return self._bind_block(psi, stream)
         ctx = self.ctx
         ctx.set_geometry(psi.gsize, psi.nw, psi.phases, psi.coords,
                          psi.dtype_code)
+        ctx.upload_links(LINKS_THIN, [u.data_ptr() for u in self.U],
+                         [u.halo_epoch.core for u in self.U], stream)
+        return ctx
+
+    def _bind_block(self, psi, stream):
+        """A field split over a process grid: after the halo exchange
+        (ensure_halo!, with the boundary phases) a rank's padded block of
+        PN + 2 nw sites holds every neighbour of its core sites, the clover
+        leaves' diagonal links included.  The kernels run on that block as a
+        lattice of its own, with no wrap phase (the ghosts carry them); the
+        core of their result is exact and its ghosts are left stale (the
+        output is marked dirty)."""
+        from .lattice import ensure_halo_
+        for u in self.U:
+            ensure_halo_(u)
+        ensure_halo_(psi)
+        ctx = self.ctx
+        box = tuple(n + 2 * psi.nw for n in psi.PN)
+        ctx.set_geometry(box, 0, (1, 1, 1, 1), (0, 0, 0, 0), psi.dtype_code)
         ctx.upload_links(LINKS_THIN, [u.data_ptr() for u in self.U],
                          [u.halo_epoch.core for u in self.U], stream)
         return ctx
@@ -120,7 +149,7 @@ class WilsonDiracOperator4D(_LinkOperator):
         return AdjointWilsonDiracOperator4D(self)
 
     def _apply(self, out, psi, dagger, precision):
-        _validate_application(out, self.U, psi, 4)
+        _validate_application(out, self.U, psi, 4, split_ok=True)
         st = _stream()
         ctx = self._bind(psi, st)
         ctx.check(ctx.lib.lmb_wilson_apply(
@@ -197,7 +226,7 @@ class WilsonDiracCloverOperator4D:
         return self.clover.refresh(tmpl)
 
     def _apply(self, out, psi, dagger, precision):
-        _validate_application(out, self.U, psi, 4)
+        _validate_application(out, self.U, psi, 4, split_ok=True)
         st = _stream()
         ctx = self.wilson._bind(psi, st)
         ctx.check(ctx.lib.lmb_wilson_clover_apply(

@@ -114,6 +114,16 @@ def cg_(x, A, b, r=None, p=None, Ap=None, *, rtol=1e-10, atol=0.0,
     if precision not in PREC:
         raise ArgumentError(f"unknown precision {precision!r}")
     native = _native_operator(A)
+    if native is not None and b.dims != (1,) * b.dim:
+        # fields split over a process grid: the reference's loop with
+        # all-reduced dots, D applied per rank block (Wilson / clover only)
+        if op_allows_blocks(native[0]) and precision == "double":
+            return _cg_generic(x, A, b, r or b.similar(), p or b.similar(),
+                               Ap or b.similar(), rtol, atol, maxiter)
+        raise ArgumentError(
+            "on a process grid cg! runs the Wilson and Wilson-clover "
+            "operators in FP64; other operators and mixed precision take one "
+            "rank per lattice")
     if native is not None:
         require_single_rank(b)
         D, op = native
@@ -198,8 +208,16 @@ def solve_evenodd_(x, D, b, *, rtol=1e-10, atol=0.0, maxiter=5000,
                     res.update_launches, res.kernel_launches, res.link_reals)
 
 
+def op_allows_blocks(D):
+    return isinstance(D, (WilsonDiracOperator4D, WilsonDiracCloverOperator4D))
+
+
 def _rdot(a: LatticeMatrix, b: LatticeMatrix) -> float:
-    return float((a.core_view().conj() * b.core_view()).sum().real)
+    local = float((a.core_view().conj() * b.core_view()).sum().real)
+    if a.dims != (1,) * a.dim:
+        from .distributed import allreduce_complex
+        return allreduce_complex(local, a.A.device).real
+    return local
 
 
 def _axpby(a, X, b, Y):

@@ -1,7 +1,7 @@
 """Process grids on CPU (gloo, 2 and 4 ranks): the halo exchange of fields
 split over PEs (exchange_dim!, LatticeMatrices_core.jl:742-921), the gather
-of the global core, the all-reduce of dot's partial sums, and the stencils
-refusing a split field.  Every rank's padded storage after set_halo! must
+of the global core, the all-reduce of dot's partial sums, and the staggered
+stencils refusing a split field.  Every rank's padded storage after set_halo! must
 equal the periodic image of the global array with the boundary phase per
 global wrap -- the single-rank ghost rule applied to the whole lattice."""
 import os
@@ -65,7 +65,9 @@ def _rank_main(rank, ws, port, dim, PEs, gsize, nw, phases, q):
         if dim == 4:
             U = [lmb.LatticeMatrix.from_array(np.asfortranarray(np.zeros((3, 3) + gsize, complex)),
                                               4, PEs, nw=nw, device="cpu") for _ in range(4)]
-            D = lmb.WilsonDiracOperator4D(U, 0.12)
+            # staggered stencils take one rank per lattice (Wilson and
+            # clover run on rank blocks: tests/test_gpu_distributed.py)
+            D = lmb.StaggeredDiracOperator4D(U, 0.1)
             try:
                 lmb.mul_(ls.similar(), D, ls)
             except lmb.ArgumentError as e:
