@@ -336,9 +336,10 @@ int lmb_gaussian_field(lmb_ctx *ctx, void *out, int ncomp, uint64_t seed,
 
 
 /* Inner product that allocates nothing: no reference counterpart.  The same
- * sum as lmb_field_dot, for callers that cannot call cudaMalloc (work
- * recorded into a CUDA graph by stream capture, pool-managed device memory
- * near its limit, loops where an allocation would synchronise the device).
+ * sum as lmb_field_dot, for callers that cannot call cudaMalloc
+ * (pool-managed device memory near its limit, host applications that forbid
+ * allocations outside their own allocator, loops where an allocation would
+ * synchronise the device).
  * No context: the geometry (L, nw, dtype as in lmb_set_geometry) is passed
  * directly, the result (Re, Im) is written to the device array out_device[2]
  * on `stream`, and nothing synchronises.  Scratch is a 1 MiB static device

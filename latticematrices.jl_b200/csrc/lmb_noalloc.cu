@@ -1,12 +1,12 @@
 // lmb_noalloc.cu -- lmb_field_dot_noalloc: the field inner product with no
 // device allocation at all.
 //
-// Who needs it: callers that must not call cudaMalloc -- code that records
-// its GPU work into a CUDA graph by stream capture (cudaMalloc is not a
-// capturable operation), callers whose device memory is owned by a pool
-// allocator (CUDA.jl, PyTorch) running close to the device limit, where a
-// stray cudaMalloc can fail or force the pool to release cached blocks, and
-// latency-sensitive loops, where cudaMalloc may synchronise the device.  Such
+// Who needs it: callers that must not call cudaMalloc -- callers whose
+// device memory is owned by a pool allocator (CUDA.jl, PyTorch) running close
+// to the device limit, where a stray cudaMalloc can fail or force the pool to
+// release cached blocks; host plugins whose embedding application forbids
+// allocations outside its own allocator; and latency-sensitive loops, where
+// cudaMalloc may synchronise the device.  Such
 // a caller cannot create an lmb_ctx either (its workspaces are allocated),
 // so this entry point takes the geometry directly and needs no context.
 //

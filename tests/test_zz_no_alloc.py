@@ -1,6 +1,7 @@
 """lmb_field_dot_noalloc: the inner product for callers that cannot allocate
-device memory (work captured into CUDA graphs, pool-managed memory near its
-limit, loops where an allocation would synchronise the device).  Its result
+device memory (pool-managed memory near its limit, host applications that
+forbid allocations outside their own allocator, loops where an allocation
+would synchronise the device).  Its result
 must equal lmb_field_dot's, call after call, although its scratch is a static
 device array shared by every call.  Collected last so that a failure here
 comes after every other test has run."""
