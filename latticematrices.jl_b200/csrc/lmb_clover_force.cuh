@@ -73,6 +73,7 @@ LMB_D void hop_outer(const Geom &g, int s, const int *c, const Field<PREC_DOUBLE
 }
 
 // stage 1: dU (36 planes, mu*9 + r + 3c) += coef * hopping-term gradient
+template <int = 0>
 __global__ void __launch_bounds__(128)
     wilson_outer_product_kernel(double2 *dU, const Field<PREC_DOUBLE, 12> dr, const Field<PREC_DOUBLE, 12> psi,
                                 const Geom g, double coef) {
@@ -131,6 +132,7 @@ LMB_D void clover_cotangent_plane(const Cx<double> *d, const Cx<double> *p, doub
 }
 
 // stage 2: dF (6 planes of 3x3) = coef sum_spin dr (G_plane psi)^+
+template <int = 0>
 __global__ void __launch_bounds__(128)
     clover_cotangent_kernel(double2 *dF, const Field<PREC_DOUBLE, 12> dr, const Field<PREC_DOUBLE, 12> psi,
                             const Geom g, double coef) {
@@ -152,6 +154,7 @@ LMB_D void mat3_mul_inplace(Cx<double> *a, const Cx<double> *b) { mat3_mul(a, b,
 
 // stage 3 for one plane (mu, nu): the links U_mu(x), U_nu(x) of site x gather
 // their occurrences in the four leaves of every anchor
+template <int = 0>
 __global__ void __launch_bounds__(64)
     clover_link_pullback_kernel(double2 *dU, const double2 *U, const double2 *dF, const Geom g, int plane,
                                 int mu, int nu) {

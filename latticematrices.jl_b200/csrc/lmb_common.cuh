@@ -7,6 +7,11 @@
 // group k for all V sites, so the 32 lanes of a warp read 32 consecutive
 // vectors (fully coalesced 128-bit loads).  Site order is the reference's
 // lexicographic order, x fastest (Latticeindices.jl:2-33).
+//
+// Build.  The library is several translation units compiled in parallel, and
+// every one of them includes these headers.  A kernel without template
+// parameters of its own is declared `template <int = 0>` so that only the
+// units that launch it compile it (launch sites need no `<>`).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>

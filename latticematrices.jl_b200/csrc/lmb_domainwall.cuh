@@ -23,6 +23,7 @@
 //         F^+(C Z).  Blocks hold floor(kDslashThreads / L5) whole 4D points.
 // Longer fifth dimensions take two passes (a local pass and a stencil pass).
 #pragma once
+#include "lmb_pack.cuh"
 #include "lmb_solver.cuh"
 
 namespace lmb {

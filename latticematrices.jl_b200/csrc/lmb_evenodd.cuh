@@ -23,6 +23,7 @@
 // V/2 sites of one parity at checkerboard index lex / 2, which needs an even
 // x extent; periodic parity needs every extent even.
 #pragma once
+#include "lmb_pack.cuh"
 #include "lmb_solver.cuh"
 
 namespace lmb {
@@ -59,6 +60,7 @@ __global__ void __launch_bounds__(256)
 // Hermitian and is stored in the same packed form.  A pivot below 1e-12 of
 // the block's largest entry counts the block as singular in *bad.
 // ---------------------------------------------------------------------------
+template <int = 0>
 __global__ void __launch_bounds__(128) clover_invert_kernel(double2 *dst, const double2 *src, int64_t V,
                                                             unsigned *bad) {
   const int64_t t = (int64_t)blockIdx.x * 128 + threadIdx.x;
@@ -295,6 +297,7 @@ __global__ void __launch_bounds__(256)
 }
 
 // |e|^2 + |o|^2 into *out
+template <int = 0>
 __global__ void __launch_bounds__(256)
     eo_norm2_kernel(const Field<PREC_DOUBLE, 12> e, const Field<PREC_DOUBLE, 12> o, int64_t Vh, double *partials,
                     unsigned *counter, double *out) {

@@ -23,6 +23,7 @@ namespace lmb {
 
 // dU_nu (+)= coef * d/dU_nu Re<dT, T_nu(M)> for the halves in `signs`
 // (1: U_nu(x) M(x+nu) U_nu(x+mu)^+, 2: U_nu(x-nu)^+ M(x-nu) U_nu(x-nu+mu))
+template <int = 0>
 __global__ void __launch_bounds__(kSmearThreads)
     transport_link_grad_kernel(double2 *dUnu, const double2 *dT, const double2 *M, const double2 *U, const Geom g,
                                int mu, int nu, int signs, double coef) {
@@ -80,6 +81,7 @@ __global__ void __launch_bounds__(kSmearThreads)
 }
 
 // y (+)= a x over n complex entries
+template <int = 0>
 __global__ void __launch_bounds__(256)
     axpy_c_kernel(double2 *y, const double2 *x, double a, int64_t n, int accumulate) {
   const int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x;
@@ -97,6 +99,7 @@ __global__ void __launch_bounds__(256)
 //   dX_mu(x) = fc eta_mu(x) [dr(x) psi(x+mu)^+ - psi(x) dr(x+mu)^+]
 //   dL_mu(x) = lc eta_mu(x) [dr(x) psi(x+3mu)^+ - psi(x) dr(x+3mu)^+]
 // dr, psi: three-component FP64 fields; neighbours carry the fermion phase.
+template <int = 0>
 __global__ void __launch_bounds__(kSmearThreads)
     hisq_outer_product_kernel(double2 *dX, double2 *dL, const Field<PREC_DOUBLE, 3> dr,
                               const Field<PREC_DOUBLE, 3> psi, const Geom g, double fc, double lc) {
@@ -136,6 +139,7 @@ __global__ void __launch_bounds__(kSmearThreads)
 // Naik pullback (HISQPullback.jl:426-459), gathered at z for direction mu:
 //   dW(z) += dL(z) (W(z+mu) W(z+2mu))^+ + W(z-mu)^+ dL(z-mu) W(z+mu)^+
 //            + (W(z-2mu) W(z-mu))^+ dL(z-2mu)
+template <int = 0>
 __global__ void __launch_bounds__(kSmearThreads)
     naik_pullback_kernel(double2 *dW, const double2 *dL, const double2 *W, const Geom g) {
   const int64_t t = (int64_t)blockIdx.x * kSmearThreads + threadIdx.x;
@@ -216,6 +220,7 @@ LMB_D void solve9(Cx<double> (*A)[9], Cx<double> *b) {
   }
 }
 
+template <int = 0>
 __global__ void __launch_bounds__(64)
     u3_pullback_kernel(double2 *dV, const double2 *dW, const double2 *Vall, int64_t n) {
   const int64_t t = (int64_t)blockIdx.x * 64 + threadIdx.x;

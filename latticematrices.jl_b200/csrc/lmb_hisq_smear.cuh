@@ -73,6 +73,7 @@ LMB_D int nb_site(const Geom &g, int s, int mu, int d) {
 }
 
 // out (+)= coef * T_nu(M) for link direction mu; signs: 1 forward, 2 backward, 3 both
+template <int = 0>
 __global__ void __launch_bounds__(kSmearThreads)
     staple_transport_kernel(double2 *out, const double2 *M, const double2 *U, const Geom g, int mu, int nu,
                             int signs, int accumulate, double coef) {
@@ -115,6 +116,7 @@ __global__ void __launch_bounds__(kSmearThreads)
 }
 
 // V_mu = c1 U_mu + c3 (S3_a+S3_b+S3_c) + c5 (S5_a+S5_b+S5_c); fields single-direction
+template <int = 0>
 __global__ void __launch_bounds__(256)
     fat7_combine_kernel(double2 *Vmu, const double2 *Umu, const double2 *s3a, const double2 *s3b,
                         const double2 *s3c, const double2 *s5a, const double2 *s5b, const double2 *s5c, int64_t V,
@@ -149,6 +151,7 @@ LMB_D void path_product_dev(const double2 *U, const Geom &g, int s, const int *p
 }
 
 // V_mu += cL sum_nu [path(nu,nu,mu,-nu,-nu) + path(-nu,-nu,mu,nu,nu)]
+template <int = 0>
 __global__ void __launch_bounds__(kSmearThreads)
     lepage_kernel(double2 *Vall, const double2 *U, const Geom g, double cL) {
   const int64_t tid = (int64_t)blockIdx.x * kSmearThreads + threadIdx.x;
@@ -221,6 +224,7 @@ LMB_D void u3_project(const Cx<double> *Vm, Cx<double> *W) {
   mat3_mul(Vm, inv, W);
 }
 
+template <int = 0>
 __global__ void __launch_bounds__(kSmearThreads)
     u3_project_kernel(double2 *W, const double2 *Vall, int64_t n) {
   const int64_t t = (int64_t)blockIdx.x * kSmearThreads + threadIdx.x;
@@ -233,6 +237,7 @@ __global__ void __launch_bounds__(kSmearThreads)
   store9(W + (size_t)mu * 9 * n, n, s, w);
 }
 
+template <int = 0>
 __global__ void __launch_bounds__(kSmearThreads)
     naik_kernel(double2 *Lall, const double2 *W, const Geom g) {
   const int64_t t = (int64_t)blockIdx.x * kSmearThreads + threadIdx.x;

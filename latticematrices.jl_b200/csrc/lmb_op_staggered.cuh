@@ -1,0 +1,84 @@
+// lmb_op_staggered.cuh -- staggered / HISQ stencil launches and their
+// operator policy.
+#pragma once
+#include "lmb_driver.cuh"
+
+namespace lmb {
+
+struct StaggeredPolicy {
+  static constexpr int NC = 3;
+  bool naik;  // HISQ: fat links X (LMB_LINKS_FAT) and Naik links L (LMB_LINKS_LONG)
+  double mass, eps;
+  int prepare(lmb_ctx *ctx, int prec, cudaStream_t st) const {
+    if (!ctx->geom_set) return fail(ctx, LMB_ERR_STATE, "lmb_set_geometry has not been called");
+    int rc = check_prec(ctx, prec);
+    if (rc) return rc;
+    if (naik) {
+      if (!ctx->links[LMB_LINKS_FAT].valid || !ctx->links[LMB_LINKS_LONG].valid)
+        return fail(ctx, LMB_ERR_STATE, "HISQ fat and long links have not been uploaded");
+      rc = ensure_link_precision(ctx, ctx->links[LMB_LINKS_FAT], prec, st, false);
+      if (rc) return rc;
+      return ensure_link_precision(ctx, ctx->links[LMB_LINKS_LONG], prec, st, false);
+    }
+    if (!ctx->links[LMB_LINKS_THIN].valid) return fail(ctx, LMB_ERR_STATE, "gauge links have not been uploaded");
+    return ensure_link_precision(ctx, ctx->links[LMB_LINKS_THIN], prec, st);
+  }
+  template <int P, int PHM, int DAG, class Epi>
+  void launch_phm(lmb_ctx *ctx, const Field<P, 3> &in, const Epi &epi, cudaStream_t st) const {
+    typedef typename Real<P>::type R;
+    const Geom &g = ctx->g;
+    const unsigned grid = grid_for(g.V, kStagThreads);
+    const R fc = (R)(DAG ? -0.5 : 0.5);
+    const R lc = (R)(DAG ? (1.0 + eps) / 48.0 : -(1.0 + eps) / 48.0);
+    if constexpr (P == PREC_SINGLE && PHM == PH_T) {
+      // x-adjacent two-site kernel: even x extent, 18-real FP32 links
+      const LinkSet &thin = ctx->links[LMB_LINKS_THIN];
+      if (ctx->pair_sites && ctx->adj_sites && g.L[0] % 2 == 0 && (naik || !thin.recon(P))) {
+        const unsigned grid2 = grid_for(g.V / 2, kStagThreads);
+        if (naik) {
+          const Gauge<P> X = gauge_view<P>(ctx->links[LMB_LINKS_FAT], g.V);
+          const Gauge<P> Lk = gauge_view<P>(ctx->links[LMB_LINKS_LONG], g.V);
+          staggered_adj_kernel<true><<<grid2, kStagThreads, 0, st>>>(g, in, X, Lk, mass, fc, lc, epi);
+        } else {
+          const Gauge<P> X = gauge_view<P>(thin, g.V);
+          staggered_adj_kernel<false><<<grid2, kStagThreads, 0, st>>>(g, in, X, X, mass, fc, lc, epi);
+        }
+        return;
+      }
+    }
+    if (naik) {
+      const Gauge<P> X = gauge_view<P>(ctx->links[LMB_LINKS_FAT], g.V);
+      const Gauge<P> Lk = gauge_view<P>(ctx->links[LMB_LINKS_LONG], g.V);
+      staggered_dslash_kernel<R, true, PHM><<<grid, kStagThreads, 0, st>>>(g, in, X, Lk, (R)mass, fc, lc, epi);
+    } else {
+      const LinkSet &ls = ctx->links[LMB_LINKS_THIN];
+      const NoLinks none{g.V};
+      if (ls.recon(P))
+        staggered_dslash_kernel<R, false, PHM><<<grid, kStagThreads, 0, st>>>(g, in, gauge12_view<P>(ls, g.V),
+                                                                               none, (R)mass, fc, lc, epi);
+      else
+        staggered_dslash_kernel<R, false, PHM><<<grid, kStagThreads, 0, st>>>(g, in, gauge_view<P>(ls, g.V),
+                                                                               none, (R)mass, fc, lc, epi);
+    }
+  }
+  template <int P, int DAG, class Epi>
+  int launch(lmb_ctx *ctx, const Field<P, 3> &in, const Epi &epi, cudaStream_t st) const {
+    // PH_T needs at most one edge crossing per hop: every extent >= 3.  The
+    // FP64 HISQ stencils measured faster on B200 with the branch form (PH_ANY).
+    const int *L = ctx->g.L;
+    if (P != PREC_DOUBLE && phase_mode_of(ctx->g.phase_mask) == PH_T && L[0] >= 3 && L[1] >= 3 && L[2] >= 3 &&
+        L[3] >= 3)
+      launch_phm<P, PH_T, DAG>(ctx, in, epi, st);
+    else
+      launch_phm<P, PH_ANY, DAG>(ctx, in, epi, st);
+    LMB_CHECK_LAUNCH(ctx);
+    return LMB_OK;
+  }
+  int link_reals(const lmb_ctx *ctx, int prec) const {
+    return (!naik && ctx->links[LMB_LINKS_THIN].recon(prec)) ? 12 : 18;
+  }
+};
+
+LMB_OP_INSTANCES(extern, StaggeredPolicy)
+
+}  // namespace lmb

@@ -75,6 +75,7 @@ __global__ void __launch_bounds__(256)
 }
 
 // 36 double2 link planes -> single / half copies
+template <int = 0>
 __global__ void __launch_bounds__(256)
     links_to_single_kernel(float4 *dst, const double2 *src, int64_t V) {
   // 36 double2 planes (mu*9 + e) -> Gauge<PREC_SINGLE>: float4 planes
@@ -93,6 +94,7 @@ __global__ void __launch_bounds__(256)
 }
 
 // k = scale exponent (|values| <= 2^k)
+template <int = 0>
 __global__ void __launch_bounds__(256)
     links_to_half_kernel(int *dst, const double2 *src, int64_t n, int k) {
   const int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x;
@@ -103,6 +105,7 @@ __global__ void __launch_bounds__(256)
 }
 
 // 36 double2 link planes (mu*9 + r + 3c) -> rows 0, 1 only (SU(3) links)
+template <int = 0>
 __global__ void __launch_bounds__(256)
     links_to_recon12_kernel(double2 *d12, float4 *f12, int4 *h12, const double2 *src, int64_t V) {
   const int64_t s = (int64_t)blockIdx.x * 256 + threadIdx.x;
@@ -126,6 +129,7 @@ __global__ void __launch_bounds__(256)
 }
 
 // max over links of |U U^+ - 1| and |det U - 1| (float bits, atomicMax)
+template <int = 0>
 __global__ void __launch_bounds__(256)
     su3_deviation_kernel(const double2 *U, int64_t V, unsigned *out_bits) {
   float m = 0.f;
@@ -157,6 +161,7 @@ __global__ void __launch_bounds__(256)
 
 // max |re|, |im| over n complex entries (one atomicMax on the float bits;
 // valid because the values are non-negative)
+template <int = 0>
 __global__ void __launch_bounds__(256)
     absmax_kernel(const double2 *src, int64_t n, unsigned *out_bits) {
   float m = 0.f;
@@ -206,6 +211,7 @@ LMB_D void mat3_adj(Cx<double> *m) {
   for (int k = 0; k < 9; k++) m[k] = t[k];
 }
 
+template <int = 0>
 __global__ void __launch_bounds__(128)
     clover_field_strength_kernel(double2 *F, const double2 *U, const Geom g) {
   const int64_t tid = (int64_t)blockIdx.x * 128 + threadIdx.x;
@@ -311,6 +317,7 @@ LMB_D void clover_blocks_site(const double2 *F, const Geom &g, int s, double coe
 }
 
 // FP64: 36 double2 planes (blk*18 + k)
+template <int = 0>
 __global__ void __launch_bounds__(128)
     clover_blocks_double_kernel(double2 *A, const double2 *F, const Geom g, double coef) {
   const int s = blockIdx.x * 128 + threadIdx.x;
@@ -320,6 +327,7 @@ __global__ void __launch_bounds__(128)
   for (int k = 0; k < 36; k++) A[k * g.V + s] = make_double2(a[2 * k], a[2 * k + 1]);
 }
 
+template <int = 0>
 __global__ void __launch_bounds__(256)
     clover_to_single_kernel(float4 *dst, const double2 *src, int64_t V) {
   const int64_t s = (int64_t)blockIdx.x * 256 + threadIdx.x;
@@ -330,6 +338,7 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+template <int = 0>
 __global__ void __launch_bounds__(256)
     clover_to_half_kernel(int4 *dst, int2 *tail, const double2 *src, int64_t V, int kexp) {
   const int64_t s = (int64_t)blockIdx.x * 256 + threadIdx.x;
