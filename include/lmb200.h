@@ -342,12 +342,16 @@ int lmb_gaussian_field(lmb_ctx *ctx, void *out, int ncomp, uint64_t seed,
  * synchronise the device).
  * No context: the geometry (L, nw, dtype as in lmb_set_geometry) is passed
  * directly, the result (Re, Im) is written to the device array out_device[2]
- * on `stream`, and nothing synchronises.  Scratch is a 1 MiB static device
- * array inside the library, so one call takes at most 16,777,216 sites
- * (LMB_ERR_ARG beyond); every call shares it, so calls that overlap on the
- * GPU (unordered streams) race.  The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress) -- make that first call
- * before any stream capture. */
+ * on `stream`, and nothing synchronises.  ncomp is 1, 3, 9 or 12 complex
+ * numbers per site (LMB_ERR_UNSUPPORTED otherwise).  Scratch is a 1 MiB
+ * static device array inside the library, so one call takes at most
+ * 16,777,216 sites (LMB_ERR_ARG beyond); every call shares it, so calls that
+ * overlap on the GPU (unordered streams) race.  Every call looks up the
+ * array's device address (cudaGetSymbolAddress, no allocation), so a device
+ * reset never leaves a stale address.  Under CUDA's lazy module loading the
+ * first call on a device loads the module that holds the array, which takes
+ * device memory: make one call per device at initialisation, before a pool
+ * allocator fills the device and outside any stream capture. */
 int lmb_field_dot_noalloc(const void *a, const void *b, const int L[4],
                           int nw, int dtype, int ncomp, double *out_device,
                           void *stream);

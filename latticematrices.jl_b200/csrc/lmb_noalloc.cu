@@ -12,17 +12,25 @@
 //
 // Scratch: the per-block partial sums and the last-block counter live in
 // one file-scope `static __device__` array of kScratchBytes (1 MiB + 256 B),
-// present on every GPU that loads liblmb200.so until the process exits.  It
-// holds one partial pair per 256-site block, so one call handles at most
-// kMaxSites = 16,777,216 lattice sites (48^3 x 96 = 10.6M fits); larger
-// volumes are rejected with LMB_ERR_ARG.  The array keeps the previous call's
-// contents; the counter is cleared on the caller's stream before every
+// held on every GPU where this file's module is loaded until the process
+// exits.  It holds one partial pair per 256-site block, so one call handles
+// at most kMaxSites = 16,777,216 lattice sites (48^3 x 96 = 10.6M fits);
+// larger volumes are rejected with LMB_ERR_ARG.  The array keeps the previous
+// call's contents; the counter is cleared on the caller's stream before every
 // launch, and every partial the kernel reads was written by the same launch.
 // All calls on a device share this one array: calls whose kernels overlap on
 // the GPU (different streams, no ordering between them) race and may return
 // wrong sums; calls on one stream, or otherwise ordered, are safe.
-#include <mutex>
-
+//
+// Module loading: with CUDA's lazy loading (the default), this file's module
+// -- its kernels and the array -- is placed on a device only when the first
+// call on that device looks up the array's address.  That load takes device
+// memory, so make one call per device at initialisation, before a pool
+// allocator has taken the free memory and outside any stream capture.
+// Later calls look the address up again (a host-side table lookup that
+// allocates nothing), so a device reset or a recreated primary context,
+// after which the module is loaded afresh and the array may move, never
+// leaves a stale address behind.
 #include "../../include/lmb200.h"
 #include "lmb_common.cuh"
 
@@ -46,23 +54,13 @@ __device__ __forceinline__ int64_t padded_offset(const PaddedGeom &pd, const int
          (int64_t)pd.P[0] * ((c[1] + pd.nw) + (int64_t)pd.P[1] * ((c[2] + pd.nw) + (int64_t)pd.P[2] * (c[3] + pd.nw)));
 }
 
-// Device addresses of g_dot_scratch, one per device, obtained once with that
-// device current.  In host code `g_dot_scratch` names a host-side shadow, not
-// device memory, so the kernel is always given the looked-up address.
-constexpr int kMaxDevices = 64;
-std::mutex g_mutex;
-void *g_scratch_ptr[kMaxDevices] = {};
-
+// Device address of g_dot_scratch on the current device.  In host code
+// `g_dot_scratch` names a host-side shadow, not device memory, so the kernel
+// is always given the looked-up address.
 int scratch_for_current_device(void **out) {
-  int dev = -1;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return LMB_ERR_CUDA;
-  std::lock_guard<std::mutex> lock(g_mutex);
-  if (!g_scratch_ptr[dev]) {
-    void *p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_dot_scratch) != cudaSuccess || !p) return LMB_ERR_CUDA;
-    g_scratch_ptr[dev] = p;
-  }
-  *out = g_scratch_ptr[dev];
+  void *p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_dot_scratch) != cudaSuccess || !p) return LMB_ERR_CUDA;
+  *out = p;
   return LMB_OK;
 }
 
