@@ -22,6 +22,9 @@ namespace lmb {
 int ensure_link_precision(lmb_ctx *ctx, LinkSet &ls, int prec, cudaStream_t st, bool allow_recon) {
   const int64_t n = 36 * ctx->g.V;
   const int64_t V = ctx->g.V;
+  if (prec != PREC_DOUBLE && !ls.finite())
+    return fail(ctx, LMB_ERR_ARG, "gauge links hold a non-finite entry (or one beyond FP32 range): "
+                "FP32 and int16 storage need finite links");
   if (allow_recon && ls.recon(prec)) {
     double2 *d = nullptr;
     float4 *f = nullptr;
@@ -60,6 +63,18 @@ int ensure_link_precision(lmb_ctx *ctx, LinkSet &ls, int prec, cudaStream_t st, 
     ls.h_version = ls.version;
   }
   return LMB_OK;
+}
+
+int resident_blocks_per_sm(const void *kern) {
+  static std::mutex mu;
+  static std::map<const void *, int> cache;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find(kern);
+  if (it != cache.end()) return it->second;
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, kDslashThreads, 0) != cudaSuccess || n < 1) n = 1;
+  cache[kern] = n;
+  return n;
 }
 
 float device_absmax(lmb_ctx *ctx, const double2 *p, int64_t n, cudaStream_t st, int *rc) {
@@ -221,6 +236,11 @@ lmb_ctx *lmb_create(int device) {
   if (const char *ps = getenv("LMB_PAIR_SITES")) ctx->pair_sites = atoi(ps) != 0;
   if (const char *as = getenv("LMB_ADJ_SITES")) ctx->adj_sites = atoi(as) != 0;
   if (const char *dw = getenv("LMB_DW_TWO_PASS")) ctx->dw_two_pass = atoi(dw) != 0;
+  if (const char *pe = getenv("LMB_PERSISTENT")) ctx->persistent = atoi(pe) != 0;
+  if (cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+    delete ctx;
+    return nullptr;
+  }
   if (cudaMalloc(&ctx->counter, sizeof(unsigned)) != cudaSuccess ||
       cudaMemset(ctx->counter, 0, sizeof(unsigned)) != cudaSuccess ||
       cudaMalloc(&ctx->st_dev, sizeof(CGState)) != cudaSuccess ||

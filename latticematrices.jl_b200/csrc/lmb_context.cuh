@@ -24,7 +24,7 @@ struct LinkSet {
   double2 *d = nullptr;  // 36 planes
   float2 *f = nullptr;
   int *h = nullptr;
-  float scale = 1.f;     // max |element| (for int16)
+  float scale = 1.f;     // max |element| (for int16); +Inf for a non-finite entry
   uint64_t f_version = ~0ull, h_version = ~0ull;
   // SU(3) links store two rows (reconstruct-12); chosen per precision by the
   // measured deviation max(|U U^+ - 1|, |det U - 1|) at upload
@@ -34,6 +34,8 @@ struct LinkSet {
   int4 *h12 = nullptr;
   uint64_t d12_version = ~0ull, f12_version = ~0ull, h12_version = ~0ull;
   bool recon(int prec) const { return prec == PREC_DOUBLE ? su3_dev <= 1e-14 : su3_dev <= 1e-6; }
+  // every entry finite and within FP32 range (the low-precision copies hold it)
+  bool finite() const { return scale <= 3.0e38f; }
 };
 
 struct CloverCache {
@@ -90,6 +92,11 @@ struct lmb_ctx {
   // the two sites of a thread are x-neighbours, read with 256-bit loads
   // (environment LMB_ADJ_SITES=0: sites s and s + V/2)
   bool adj_sites = true;
+  // int16 K1 / K2 stencils as persistent kernels (one block per resident
+  // slot walking the tiles, one reduction per block); LMB_PERSISTENT=0 in
+  // the environment: one block per tile
+  bool persistent = true;
+  int sm_count = 0;
   lmb::LinkSet links[3];
   // domain-wall operator (lmb_domainwall_set): L5 slices of the 4D geometry,
   // mass, M and the coefficients a, b, c (3 L5 doubles, device memory)

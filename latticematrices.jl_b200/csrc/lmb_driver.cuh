@@ -114,7 +114,12 @@ int cg_run(lmb_ctx *ctx, const lmb_cg_params *prm, const Op &op, void *x_pad, co
     return fail(ctx, LMB_ERR_CUDA, "out of device memory (reduction partials)");
   rc = op.prepare(ctx, PREC_DOUBLE, st);
   if (rc) return rc;
-  if (mixed) {
+  // Links with a non-finite entry make D x non-finite for every x, so the
+  // initial FP64 residual b - D'D x breaks the solve down at iteration 0 with
+  // a NaN residual, as the reference's cg! does (cg.jl:93-104); the
+  // low-precision copies are never built or used then.
+  const bool finite_links = op.links_finite(ctx);
+  if (mixed && finite_links) {
     rc = op.prepare(ctx, PS, st);
     if (rc) return rc;
   }
@@ -140,7 +145,8 @@ int cg_run(lmb_ctx *ctx, const lmb_cg_params *prm, const Op &op, void *x_pad, co
   nl++;
   rc = read_state(ctx, st);
   if (rc) return rc;
-  const bool zero_guess = ctx->st_host->xx == 0.0;
+  // b - D'D 0 = b needs finite links (NaN * 0 is NaN)
+  const bool zero_guess = ctx->st_host->xx == 0.0 && finite_links;
   // r = b - D'D x (FP64)
   auto true_residual = [&](int mode) -> int {
     EpiStore<PREC_DOUBLE, NC> e1{t64, nullptr};
@@ -168,6 +174,8 @@ int cg_run(lmb_ctx *ctx, const lmb_cg_params *prm, const Op &op, void *x_pad, co
   CGState *hs = ctx->st_host;
   if (!std::isfinite(hs->bb)) hs->status = ST_BREAKDOWN;
   if (hs->status == ST_RUNNING && prm->maxiter == 0) hs->status = ST_MAXITER;
+  if (mixed && !finite_links && hs->status == ST_RUNNING)  // finite in FP64, beyond FP32 range
+    return fail(ctx, LMB_ERR_ARG, "gauge links lie beyond FP32 range: solve with FP64 fields");
   if (hs->status != ST_RUNNING)
     LMB_CUDA(ctx, cudaMemcpyAsync(ctx->st_dev, hs, sizeof(CGState), cudaMemcpyHostToDevice, st));
 

@@ -6,6 +6,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -17,6 +19,16 @@ namespace lmb {
 inline cudaStream_t as_stream(void *s) { return (cudaStream_t)s; }
 
 inline bool ctx_ok(lmb_ctx *ctx) { return ctx != nullptr; }
+
+// blocks of kernel `kern` (kDslashThreads threads, no dynamic shared memory)
+// resident on the whole device at once: the grid of a persistent launch.
+// The per-SM figure depends only on the kernel and the architecture, so it
+// is looked up once per kernel (lmb_capi.cu).
+int resident_blocks_per_sm(const void *kern);
+template <class K>
+unsigned resident_grid(const lmb_ctx *ctx, K kern) {
+  return (unsigned)(resident_blocks_per_sm((const void *)kern) * (ctx->sm_count > 0 ? ctx->sm_count : 1));
+}
 
 inline int check_prec(lmb_ctx *ctx, int prec) {
   if (prec < PREC_DOUBLE || prec > PREC_HALF) return fail(ctx, LMB_ERR_ARG, "unknown precision %d", prec);

@@ -66,6 +66,7 @@ struct DWPolicy {
     return launch_g<P, DAG>(ctx, in, gauge_view<P>(ls, ctx->g.V), epi, st);
   }
   int link_reals(const lmb_ctx *ctx, int prec) const { return ctx->links[LMB_LINKS_THIN].recon(prec) ? 12 : 18; }
+  bool links_finite(const lmb_ctx *ctx) const { return ctx->links[LMB_LINKS_THIN].finite(); }
 };
 
 inline int64_t op_volume(const lmb_ctx *ctx, const DWPolicy &) { return ctx->g.V * ctx->dw_L5; }

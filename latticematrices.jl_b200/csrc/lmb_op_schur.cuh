@@ -102,6 +102,7 @@ struct SchurPolicy {
     return launch_g<P, DAG>(ctx, in, eo_gauge_view<P>(ctx), epi, st);
   }
   int link_reals(const lmb_ctx *ctx, int prec) const { return ctx->links[LMB_LINKS_THIN].recon(prec) ? 12 : 18; }
+  bool links_finite(const lmb_ctx *ctx) const { return ctx->links[LMB_LINKS_THIN].finite(); }
 };
 
 // the CG driver's b and x of the Schur system are FP64 half fields of the

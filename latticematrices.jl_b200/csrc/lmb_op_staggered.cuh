@@ -77,6 +77,10 @@ struct StaggeredPolicy {
   int link_reals(const lmb_ctx *ctx, int prec) const {
     return (!naik && ctx->links[LMB_LINKS_THIN].recon(prec)) ? 12 : 18;
   }
+  bool links_finite(const lmb_ctx *ctx) const {
+    if (naik) return ctx->links[LMB_LINKS_FAT].finite() && ctx->links[LMB_LINKS_LONG].finite();
+    return ctx->links[LMB_LINKS_THIN].finite();
+  }
 };
 
 LMB_OP_INSTANCES(extern, StaggeredPolicy)

@@ -15,8 +15,16 @@ void launch_wilson_cl(lmb_ctx *ctx, const Field<PS, 12> &in, const G &U, const C
   const Geom &g = ctx->g;
   if constexpr (PS == PREC_HALF && std::is_same<G, Gauge12<PREC_HALF>>::value) {
     if (ctx->pair_sites && ctx->adj_sites && g.L[0] % 2 == 0) {
-      wilson_half_adj_kernel<DAG, CLOVER, PHM><<<grid_for(g.V / 2, kDslashThreads), kDslashThreads, 0, st>>>(
-          g, in, U, A, (float)kappa, epi);
+      const unsigned ntiles = grid_for(g.V / 2, kDslashThreads);
+      if constexpr (PersistentEpi<Epi>::value) {
+        if (ctx->persistent) {
+          auto kern = wilson_half_adj_persistent_kernel<DAG, CLOVER, PHM, CL, Epi>;
+          const unsigned grid = std::min(ntiles, resident_grid(ctx, kern));
+          kern<<<grid, kDslashThreads, 0, st>>>(g, in, U, A, (float)kappa, epi, (int)ntiles);
+          return;
+        }
+      }
+      wilson_half_adj_kernel<DAG, CLOVER, PHM><<<ntiles, kDslashThreads, 0, st>>>(g, in, U, A, (float)kappa, epi);
       return;
     }
   }
@@ -82,6 +90,7 @@ struct WilsonPolicy {
     return launch_wilson<P, P, false, DAG>(ctx, in, kappa, epi, st);
   }
   int link_reals(const lmb_ctx *ctx, int prec) const { return ctx->links[LMB_LINKS_THIN].recon(prec) ? 12 : 18; }
+  bool links_finite(const lmb_ctx *ctx) const { return ctx->links[LMB_LINKS_THIN].finite(); }
 };
 
 LMB_OP_INSTANCES(extern, WilsonPolicy)

@@ -160,14 +160,17 @@ __global__ void __launch_bounds__(256)
 }
 
 // max |re|, |im| over n complex entries (one atomicMax on the float bits;
-// valid because the values are non-negative)
+// valid because the values are non-negative).  A NaN entry counts as +Inf
+// (fmaxf would drop it), so the result is finite exactly when every entry
+// is finite and within FP32 range.
 template <int = 0>
 __global__ void __launch_bounds__(256)
     absmax_kernel(const double2 *src, int64_t n, unsigned *out_bits) {
   float m = 0.f;
   for (int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x; i < n; i += (int64_t)gridDim.x * 256) {
     const double2 t = src[i];
-    m = fmaxf(m, fmaxf(fabsf((float)t.x), fabsf((float)t.y)));
+    const float a = fmaxf(fabsf((float)t.x), fabsf((float)t.y));
+    m = fmaxf(m, (isnan(t.x) || isnan(t.y)) ? INFINITY : a);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));

@@ -107,6 +107,15 @@ LMB_D Cx2 dec_pair2(int w0, int w1, unsigned y0, unsigned y1, float2 negc) {
   return Cx2(lo + negc, hi + negc);
 }
 
+// The same two words without the offset subtraction: the floats hold
+// value + c, c = base (1 + 2^-8) of the word's site (see project_raw)
+LMB_D Cx2 raw_pair2(int w0, int w1, unsigned y0, unsigned y1) {
+  return Cx2(make_float2(__uint_as_float(__byte_perm((unsigned)w0, y0, 0x5410u)),
+                         __uint_as_float(__byte_perm((unsigned)w1, y1, 0x5410u))),
+             make_float2(__uint_as_float(__byte_perm((unsigned)w0, y0, 0x5432u)),
+                         __uint_as_float(__byte_perm((unsigned)w1, y1, 0x5432u))));
+}
+
 // Encoding exponent of a site: the smallest e with m (1 + 2^-15) < 2^e, so
 // that |v| 2^(15-e) < 32768 / (1 + 2^-15) and rint() of it never exceeds
 // 32767: no clamp is needed.  e is clamped to [-100, 110]: a site whose
@@ -371,6 +380,40 @@ LMB_D void store_adj(const Field<PREC_SINGLE, NC> &f, int64_t s, const Cx2 *v) {
                                  two ? v[2 * k + 1].im.y : 0.f);
     st256(reinterpret_cast<int4 *>(f.data + k * f.V + s), *reinterpret_cast<const int4 *>(&a),
           *reinterpret_cast<const int4 *>(&b));
+  }
+}
+
+// raw words (value + c per lane) of the two sites s, s + 1 (s even) and of
+// two arbitrary sites; nc2 = -2c per lane
+template <int NC>
+LMB_D void load_adj_raw(const Field<PREC_HALF, NC> &f, int64_t s, Cx2 *v, float2 &nc2) {
+  const float2 nb = __ldg(reinterpret_cast<const float2 *>(f.norm + s));
+  const unsigned y0 = __float_as_uint(nb.x) >> 16, y1 = __float_as_uint(nb.y) >> 16;
+  nc2 = make_float2(-nb.x * 2.0078125f, -nb.y * 2.0078125f);
+  constexpr int P = Field<PREC_HALF, NC>::kPlanes;
+#pragma unroll
+  for (int k = 0; k < P; k++) {
+    int4 t0, t1;
+    ld256(f.data + k * f.V + s, t0, t1);
+    const int w0[4] = {t0.x, t0.y, t0.z, t0.w}, w1[4] = {t1.x, t1.y, t1.z, t1.w};
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      if (4 * k + j < NC) v[4 * k + j] = raw_pair2(w0[j], w1[j], y0, y1);
+  }
+}
+template <int NC>
+LMB_D void load2_raw(const Field<PREC_HALF, NC> &f, int64_t s0, int64_t s1, Cx2 *v, float2 &nc2) {
+  const float b0 = __ldg(f.norm + s0), b1 = __ldg(f.norm + s1);
+  const unsigned y0 = __float_as_uint(b0) >> 16, y1 = __float_as_uint(b1) >> 16;
+  nc2 = make_float2(-b0 * 2.0078125f, -b1 * 2.0078125f);
+  constexpr int P = Field<PREC_HALF, NC>::kPlanes;
+#pragma unroll
+  for (int k = 0; k < P; k++) {
+    const int4 t0 = __ldg(f.data + k * f.V + s0), t1 = __ldg(f.data + k * f.V + s1);
+    const int w0[4] = {t0.x, t0.y, t0.z, t0.w}, w1[4] = {t1.x, t1.y, t1.z, t1.w};
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      if (4 * k + j < NC) v[4 * k + j] = raw_pair2(w0[j], w1[j], y0, y1);
   }
 }
 

@@ -367,6 +367,48 @@ __global__ void __launch_bounds__(kDslashThreads, LMB_PAIR_MINB)
 }
 
 // ---------------------------------------------------------------------------
+// (1 + PM g_mu) psi straight from the raw int16 words of psi: a raw float is
+// psi + c with c = base (1 + 2^-8) of its site (lmb_pair.cuh), so a
+// difference of two raw values is psi_a - psi_b and a sum is
+// (raw_a - 2c) + raw_b.  Every step is exact: operands and results are
+// integers times the site's quantum 2^(e-15) below 2^24 in magnitude, so h
+// equals project() of the decoded spinor bit for bit, with 2 or 3 FADD2 per
+// complex entry of h instead of 6.  nc2 = -2c per lane.
+// ---------------------------------------------------------------------------
+template <int SIG>
+LMB_D float2 raw_comb(float2 a, float2 b, float2 nc2) {
+  if constexpr (SIG > 0) return (a + nc2) + b;
+  else return a - b;
+}
+// a + SIG * b (IM = false) or a + SIG * i b (IM = true), a and b raw
+template <int SIG, bool IM>
+LMB_D Cx2 raw_term(const Cx2 &a, const Cx2 &b, float2 nc2) {
+  if constexpr (IM) return Cx2(raw_comb<-SIG>(a.re, b.im, nc2), raw_comb<SIG>(a.im, b.re, nc2));
+  else return Cx2(raw_comb<SIG>(a.re, b.re, nc2), raw_comb<SIG>(a.im, b.im, nc2));
+}
+// the rows of project<PM, MU> on raw words
+template <int PM, int MU>
+LMB_D void project_raw(const Cx2 *p, float2 nc2, Cx2 *h) {
+  constexpr int S = PM > 0 ? 1 : -1;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    if constexpr (MU == 0) {
+      h[c] = raw_term<-S, true>(p[c], p[c + 9], nc2);
+      h[c + 3] = raw_term<-S, true>(p[c + 3], p[c + 6], nc2);
+    } else if constexpr (MU == 1) {
+      h[c] = raw_term<-S, false>(p[c], p[c + 9], nc2);
+      h[c + 3] = raw_term<S, false>(p[c + 3], p[c + 6], nc2);
+    } else if constexpr (MU == 2) {
+      h[c] = raw_term<-S, true>(p[c], p[c + 6], nc2);
+      h[c + 3] = raw_term<S, true>(p[c + 3], p[c + 9], nc2);
+    } else {
+      h[c] = raw_term<-S, false>(p[c], p[c + 6], nc2);
+      h[c + 3] = raw_term<-S, false>(p[c + 3], p[c + 9], nc2);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // int16 storage, reconstruct-12 links: lanes are x-adjacent sites s0 = 2i
 // (x even) and s1 = s0 + 1 (lmb_pair.cuh: one 256-bit load per plane serves
 // both).  y, z, t hops and the site's own links, spinor and clover use those
@@ -379,17 +421,18 @@ LMB_D void hop_adj(const Geom &g, int s0, const int *c0, const int *c1, const Fi
   constexpr int BPM = -FPM;
   const bool ph = (g.phase_mask >> MU) & 1;
   Cx2 p[12], h[6], uh[6], u[9];
+  float2 nc2;
   {
     int w0, w1;
     if constexpr (MU == 0) {
       w0 = 0;  // x + 1 of an even x never crosses the edge
       const int n1 = fwd_site(g, s0 + 1, c1, 0, 1, &w1);
-      load2(in, s0 + 1, n1, p);
+      load2_raw(in, s0 + 1, n1, p, nc2);
     } else {
-      load_adj(in, fwd_site(g, s0, c0, MU, 1, &w0), p);
+      load_adj_raw(in, fwd_site(g, s0, c0, MU, 1, &w0), p, nc2);
       w1 = w0;
     }
-    project<FPM, MU>(p, h);
+    project_raw<FPM, MU>(p, nc2, h);
     if constexpr (PHM == PH_ANY) {
       if (ph && (w0 | w1)) phase2(h, g.ph_fwd[MU], w0, w1);
     } else if constexpr (MU == 3) {
@@ -404,8 +447,8 @@ LMB_D void hop_adj(const Geom &g, int s0, const int *c0, const int *c1, const Fi
     if constexpr (MU == 0) {
       const int n0 = bwd_site(g, s0, c0, 0, 1, &w0);
       w1 = 0;  // x - 1 of an odd x never crosses the edge
-      load2(in, n0, s0, p);
-      project<BPM, MU>(p, h);
+      load2_raw(in, n0, s0, p, nc2);
+      project_raw<BPM, MU>(p, nc2, h);
       if constexpr (PHM == PH_ANY) {
         if (ph && (w0 | w1)) phase2(h, g.ph_bwd[MU], w0, w1);
       }
@@ -413,8 +456,8 @@ LMB_D void hop_adj(const Geom &g, int s0, const int *c0, const int *c1, const Fi
     } else {
       const int n0 = bwd_site(g, s0, c0, MU, 1, &w0);
       w1 = w0;
-      load_adj(in, n0, p);
-      project<BPM, MU>(p, h);
+      load_adj_raw(in, n0, p, nc2);
+      project_raw<BPM, MU>(p, nc2, h);
       if constexpr (PHM == PH_ANY) {
         if (ph && (w0 | w1)) phase2(h, g.ph_bwd[MU], w0, w1);
       } else if constexpr (MU == 3) {
@@ -424,6 +467,42 @@ LMB_D void hop_adj(const Geom &g, int s0, const int *c0, const int *c1, const Fi
     }
     su3_adj_mul_half(u, h, uh);
     reconstruct<BPM, MU>(acc, uh);
+  }
+}
+
+// D psi (or D^+ psi) at the x-adjacent sites s0 (x even) and s0 + 1
+template <int DAG, bool CLOVER, int PHM, class CL>
+LMB_D void half_adj_sites(const Geom &g, int s0, const Field<PREC_HALF, 12> &in, const Gauge12<PREC_HALF> &U,
+                          const CL &A, float kappa, Cx2 *out) {
+  int c0[4], c1[4];
+  site_coords(g, s0, c0);
+  c1[0] = c0[0] + 1;
+  c1[1] = c0[1];
+  c1[2] = c0[2];
+  c1[3] = c0[3];
+  Cx2 acc[12];
+#pragma unroll
+  for (int k = 0; k < 12; k++) acc[k] = cx2_zero();
+  hop_adj<DAG, 0, PHM>(g, s0, c0, c1, in, U, acc);
+  hop_adj<DAG, 1, PHM>(g, s0, c0, c1, in, U, acc);
+  hop_adj<DAG, 2, PHM>(g, s0, c0, c1, in, U, acc);
+  hop_adj<DAG, 3, PHM>(g, s0, c0, c1, in, U, acc);
+  Cx2 p[12];
+  load_adj(in, s0, p);
+  const float2 k2 = f2(kappa);
+  if constexpr (CLOVER) {
+    float2 a[36];
+    Cx2 o[6];
+#pragma unroll
+    for (int blk = 0; blk < 2; blk++) {
+      load_adj(A, blk, s0, a);
+      herm6_mul(a, p + 6 * blk, o);
+#pragma unroll
+      for (int k = 0; k < 6; k++) out[6 * blk + k] = cfms_real(k2, acc[6 * blk + k], o[k]);
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 12; k++) out[k] = cfms_real(k2, acc[k], p[k]);
   }
 }
 
@@ -438,39 +517,33 @@ __global__ void __launch_bounds__(kDslashThreads, LMB_PAIR_MINB)
   const bool active = i < (int)(g.V >> 1);
   const int s0 = 2 * i;
   Cx2 out[12];
-  if (active) {
-    int c0[4], c1[4];
-    site_coords(g, s0, c0);
-    c1[0] = c0[0] + 1;
-    c1[1] = c0[1];
-    c1[2] = c0[2];
-    c1[3] = c0[3];
-    Cx2 acc[12];
-#pragma unroll
-    for (int k = 0; k < 12; k++) acc[k] = cx2_zero();
-    hop_adj<DAG, 0, PHM>(g, s0, c0, c1, in, U, acc);
-    hop_adj<DAG, 1, PHM>(g, s0, c0, c1, in, U, acc);
-    hop_adj<DAG, 2, PHM>(g, s0, c0, c1, in, U, acc);
-    hop_adj<DAG, 3, PHM>(g, s0, c0, c1, in, U, acc);
-    Cx2 p[12];
-    load_adj(in, s0, p);
-    const float2 k2 = f2(kappa);
-    if constexpr (CLOVER) {
-      float2 a[36];
-      Cx2 o[6];
-#pragma unroll
-      for (int blk = 0; blk < 2; blk++) {
-        load_adj(A, blk, s0, a);
-        herm6_mul(a, p + 6 * blk, o);
-#pragma unroll
-        for (int k = 0; k < 6; k++) out[6 * blk + k] = cfms_real(k2, acc[6 * blk + k], o[k]);
-      }
-    } else {
-#pragma unroll
-      for (int k = 0; k < 12; k++) out[k] = cfms_real(k2, acc[k], p[k]);
-    }
-  }
+  if (active) half_adj_sites<DAG, CLOVER, PHM>(g, s0, in, U, A, kappa, out);
   epi.pair_adj(s0, active, out);
+}
+
+// Persistent form for the reducing CG epilogues: gridDim.x blocks (the
+// device's resident blocks) walk the tiles of kDslashThreads pairs
+// t = blockIdx.x, blockIdx.x + gridDim.x, ... in a fixed order.  The
+// epilogue carries its reduction in registers across the tiles
+// (pair_adj_acc) and reduces once per block at the end (finish), so no block
+// waits at a barrier or on the grid counter between tiles, and the result
+// does not depend on timing.
+template <int DAG, bool CLOVER, int PHM, class CL, class Epi>
+__global__ void __launch_bounds__(kDslashThreads, LMB_PAIR_MINB)
+    wilson_half_adj_persistent_kernel(const Geom g, const Field<PREC_HALF, 12> in, const Gauge12<PREC_HALF> U,
+                                      const CL A, const float kappa, Epi epi, int ntiles) {
+  if (epi.skip()) return;
+  double red[1] = {0.0};
+  const int npairs = (int)(g.V >> 1);
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int i = tile * kDslashThreads + threadIdx.x;
+    const bool active = i < npairs;
+    const int s0 = 2 * i;
+    Cx2 out[12];
+    if (active) half_adj_sites<DAG, CLOVER, PHM>(g, s0, in, U, A, kappa, out);
+    epi.pair_adj_acc(s0, active, out, red);
+  }
+  epi.finish(red);
 }
 
 }  // namespace lmb
