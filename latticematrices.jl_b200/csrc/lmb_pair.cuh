@@ -519,6 +519,22 @@ LMB_D void load_adj(const Gauge<PREC_SINGLE> &U, int mu, int64_t s, Cx2 *u) {
   u[8] = Cx2(f2(c.x, c.z), f2(c.y, c.w));
 }
 
+// o += A v, A Hermitian 6x6 (6 real diagonal, 15 complex lower entries)
+LMB_D void herm6_mul_acc(const float2 *a, const Cx2 *v, Cx2 *o) {
+#pragma unroll
+  for (int i = 0; i < 6; i++) o[i] = Cx2(fma2(a[i], v[i].re, o[i].re), fma2(a[i], v[i].im, o[i].im));
+  int k = 6;
+#pragma unroll
+  for (int i = 1; i < 6; i++)
+#pragma unroll
+    for (int j = 0; j < i; j++) {
+      const Cx2 aij(a[k], a[k + 1]);
+      o[i] = cfma(aij, v[j], o[i]);
+      o[j] = cfma_conj(aij, v[i], o[j]);
+      k += 2;
+    }
+}
+
 // Hermitian 6x6 (6 real diagonal, 15 complex lower entries) times a 6-vector
 LMB_D void herm6_mul(const float2 *a, const Cx2 *v, Cx2 *o) {
 #pragma unroll

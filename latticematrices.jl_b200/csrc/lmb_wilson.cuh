@@ -480,29 +480,29 @@ LMB_D void half_adj_sites(const Geom &g, int s0, const Field<PREC_HALF, 12> &in,
   c1[1] = c0[1];
   c1[2] = c0[2];
   c1[3] = c0[3];
-  Cx2 acc[12];
+  // out = -kappa * hopping sum, then A psi accumulated into it (no separate
+  // A psi array is live)
 #pragma unroll
-  for (int k = 0; k < 12; k++) acc[k] = cx2_zero();
-  hop_adj<DAG, 0, PHM>(g, s0, c0, c1, in, U, acc);
-  hop_adj<DAG, 1, PHM>(g, s0, c0, c1, in, U, acc);
-  hop_adj<DAG, 2, PHM>(g, s0, c0, c1, in, U, acc);
-  hop_adj<DAG, 3, PHM>(g, s0, c0, c1, in, U, acc);
+  for (int k = 0; k < 12; k++) out[k] = cx2_zero();
+  hop_adj<DAG, 0, PHM>(g, s0, c0, c1, in, U, out);
+  hop_adj<DAG, 1, PHM>(g, s0, c0, c1, in, U, out);
+  hop_adj<DAG, 2, PHM>(g, s0, c0, c1, in, U, out);
+  hop_adj<DAG, 3, PHM>(g, s0, c0, c1, in, U, out);
   Cx2 p[12];
   load_adj(in, s0, p);
-  const float2 k2 = f2(kappa);
+  const float2 nk2 = f2(-kappa);
   if constexpr (CLOVER) {
+#pragma unroll
+    for (int k = 0; k < 12; k++) out[k] = Cx2(nk2 * out[k].re, nk2 * out[k].im);
     float2 a[36];
-    Cx2 o[6];
 #pragma unroll
     for (int blk = 0; blk < 2; blk++) {
       load_adj(A, blk, s0, a);
-      herm6_mul(a, p + 6 * blk, o);
-#pragma unroll
-      for (int k = 0; k < 6; k++) out[6 * blk + k] = cfms_real(k2, acc[6 * blk + k], o[k]);
+      herm6_mul_acc(a, p + 6 * blk, out + 6 * blk);
     }
   } else {
 #pragma unroll
-    for (int k = 0; k < 12; k++) out[k] = cfms_real(k2, acc[k], p[k]);
+    for (int k = 0; k < 12; k++) out[k] = Cx2(fma2(nk2, out[k].re, p[k].re), fma2(nk2, out[k].im, p[k].im));
   }
 }
 
