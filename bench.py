@@ -94,8 +94,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
     ap.add_argument("--workload", default="clover",
-                    choices=["clover", "wilson8", "hisq", "batched", "force", "clover_force", "dw",
-                             "evenodd"],
+                    choices=["clover", "wilson8", "hisq", "hisq_dslash", "batched", "force",
+                             "clover_force", "dw", "evenodd"],
                     help="clover: 32^3x64 Wilson-clover mixed vs FP64 CG (the "
                          "headline line); wilson8: 8^4 Wilson FP64 CG beside the "
                          "CPU oracle; hisq: 48^3x96 HISQ smearing + CG; batched: "
@@ -104,7 +104,8 @@ def parse():
                          "clover_force: 24^4 Wilson-clover fermion force, same check; "
                          "dw: 16^3x32 x L5 12 Mobius domain-wall D5'D5 CG; evenodd: "
                          "32^3x64 clover D x = b, even/odd Schur solve vs the "
-                         "D'D CG route")
+                         "D'D CG route; hisq_dslash: one FP64 HISQ D application "
+                         "at 8^4 .. 32^4 beside the reference's published table")
     ap.add_argument("--l5", type=int, default=12)
     ap.add_argument("--fd-directions", type=int, default=64)
     return ap.parse_args()
@@ -573,6 +574,72 @@ def run_hisq(args):
     print(json.dumps(out), flush=True)
 
 
+# The reference's published HISQ Dslash table (one H100 NVL, FP64, m 0,
+# eps_N -0.083, antiperiodic t; ms per full-lattice application, median):
+# LatticeMatrices v1.1.0 and SIMULATeQCD 767a1b1
+# (benchmark/HISQ_DIRAC_BENCHMARK_2026-08-17.md:66-69)
+HISQ_PUBLISHED_MS = {8: (0.11104, 0.01431), 16: (0.18496, 0.05011),
+                     24: (0.64086, 0.24036), 32: (2.56497, 0.70998)}
+
+
+def run_hisq_dslash(args):
+    """One full-lattice HISQ D application, FP64, m 0, eps_N -0.083,
+    antiperiodic t, at 8^4, 16^4, 24^4 and 32^4, smearing excluded, with the
+    reference's protocol (input and output swapped after every application,
+    median of 9 samples; benchmark/HISQ_DIRAC_BENCHMARK_2026-08-17.md:10-40).
+    `resident`: the stencil on the library's resident fields (what one Krylov
+    iteration pays); `api`: mul! through the public API on padded fields,
+    which adds the layout conversion of input and output.  Links exp(0.25 i H)
+    seed 1 (deterministic), Gaussian source seed 2.  Algorithmic bytes per
+    site: 8 links x 18 reals + in + out = 156 reals (1248 B FP64, 624 B FP32)."""
+    import torch
+    import lmb200 as lmb
+    peak, peak_kind = measured_peak()
+    st = torch.cuda.current_stream()
+    rows = []
+    for n in (8, 16, 24, 32):
+        L = (n, n, n, n)
+        sites = n ** 4
+        U = lmb.random_su3_links(L, 0.25, 1, nw=3)
+        links = lmb.hisq_links_from_thin(U, -0.083)
+        D = lmb.HISQDiracOperator4D(links, 0.0, -0.083)
+        psi = lmb.gaussian_fermion(L, 3, 1, 2, nw=3, phases=PHASES)
+        out = psi.similar()
+        napply = max(20, min(2000, int(2e8 // sites)))
+        row = {"L": n, "sites": sites, "napply_per_sample": napply}
+        for prec, rb in (("double", 8), ("single", 4)):
+            samples = [lmb.operator_timing(D, psi, napply, precision=prec) for _ in range(9)]
+            ms = statistics.median(samples)
+            gbs = 156 * rb * sites / (ms * 1e-3) / 1e9
+            row[prec] = {"resident_ms_median": ms, "resident_ms_min": min(samples),
+                         "gbs": gbs, "hbm_frac": gbs / peak}
+        # public API, FP64: mul!(out, D, psi), swapping the two fields
+        a, b = psi, out
+        for _ in range(3):
+            lmb.mul_(b, D, a)
+            a, b = b, a
+        samples = []
+        for _ in range(9):
+            k = max(5, napply // 4)
+            def loop():
+                nonlocal a, b
+                for _ in range(k):
+                    lmb.mul_(b, D, a)
+                    a, b = b, a
+            _, sec = _timed(loop, st)
+            samples.append(sec * 1e3 / k)
+        row["double"]["api_ms_median"] = statistics.median(samples)
+        lm, sq = HISQ_PUBLISHED_MS[n]
+        row["published_h100_ms"] = {"latticematrices_median": lm, "simulateqcd_median": sq}
+        row["speedup_vs_latticematrices_h100"] = lm / row["double"]["resident_ms_median"]
+        rows.append(row)
+        del U, links, D, psi, out, a, b
+        torch.cuda.empty_cache()
+    print(json.dumps({"workload": "HISQ Dslash FP64, m 0, eps_N -0.083, antiperiodic t, one full-lattice "
+                                  "application (smearing excluded)",
+                      "peak_gbs": peak, "peak_kind": peak_kind, "rows": rows}), flush=True)
+
+
 def run_batched(args):
     """16 Gaussian right-hand sides of Wilson D'D on 32^4 plus
     lattices 8^4 x4, 12^4 x4, 16^4 x2, 24^4 x1, in one batched solve (FP32
@@ -850,7 +917,7 @@ def main():
     else:
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        {"wilson8": run_wilson8, "hisq": run_hisq, "batched": run_batched,
+        {"wilson8": run_wilson8, "hisq": run_hisq, "hisq_dslash": run_hisq_dslash, "batched": run_batched,
          "force": run_force, "clover_force": run_clover_force, "dw": run_dw,
          "evenodd": run_evenodd}[args.workload](args)
 

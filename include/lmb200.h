@@ -314,6 +314,20 @@ int lmb_cg_ddagd_batched(lmb_ctx *ctx, const lmb_cg_params *params,
                          lmb_cg_result *results, lmb_batch_tuning *tuning,
                          void *stream);
 
+/* Application rate of an operator on the library's resident fields: no
+ * reference counterpart (it replaces the timing loop of
+ * benchmark/hisq_dirac_scaling.jl:82-100, which times mul! on one pair of
+ * fields).  `in` (padded layout) is packed once; the operator of params->op
+ * (kappa / csw / mass / naik_epsilon of params, domain wall as set by
+ * lmb_domainwall_set) is then applied 2 + napply times between two internal
+ * fields at params->precision, input and output swapped after every
+ * application; *ms_per_apply is the device time of the last napply
+ * applications divided by napply (CUDA events on `stream`).  Synchronises
+ * the stream. */
+int lmb_operator_timing(lmb_ctx *ctx, const lmb_cg_params *params,
+                        const void *in, int napply, int dagger,
+                        double *ms_per_apply, void *stream);
+
 /* dot(a, b) = sum conj(a) b over the core (LinearAlgebras/linearalgebra_D.jl:
  * 3325-3341) of two padded fields with ncomp complex numbers per site.
  * out[0] = Re, out[1] = Im.  Synchronises the stream. */

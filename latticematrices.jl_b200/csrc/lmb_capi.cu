@@ -65,6 +65,35 @@ int ensure_link_precision(lmb_ctx *ctx, LinkSet &ls, int prec, cudaStream_t st, 
   return LMB_OK;
 }
 
+// The link sets and clover caches are sized by the volume they were built
+// for: free them (the next use rebuilds them) when that volume goes away.
+// Version counters keep counting across a release, so nothing keyed by an
+// old version (parity-ordered copies, derived caches) can match again.
+void release_site_caches(lmb_ctx *ctx) {
+  for (auto &ls : ctx->links) {
+    cudaFree(ls.d);
+    cudaFree(ls.f);
+    cudaFree(ls.h);
+    cudaFree(ls.d12);
+    cudaFree(ls.f12);
+    cudaFree(ls.h12);
+    const uint64_t version = ls.version + 1;
+    ls = LinkSet{};
+    ls.version = version;
+  }
+  for (CloverCache *cc : {&ctx->clover, &ctx->clover_inv}) {
+    cudaFree(cc->F);
+    cudaFree(cc->d);
+    cudaFree(cc->f);
+    cudaFree(cc->h);
+    cudaFree(cc->ht);
+    const uint64_t dv = cc->d_version + 1;
+    *cc = CloverCache{};
+    cc->d_version = dv;
+  }
+  ctx->smear.valid = false;
+}
+
 int resident_blocks_per_sm(const void *kern) {
   static std::mutex mu;
   static std::map<const void *, int> cache;
@@ -260,24 +289,8 @@ void lmb_destroy(lmb_ctx *ctx) {
     cudaFree(bl.d12);
     cudaFree(bl.f12);
   }
-  for (auto &ls : ctx->links) {
-    cudaFree(ls.d);
-    cudaFree(ls.f);
-    cudaFree(ls.h);
-    cudaFree(ls.d12);
-    cudaFree(ls.f12);
-    cudaFree(ls.h12);
-  }
-  cudaFree(ctx->clover.F);
-  cudaFree(ctx->clover.d);
+  release_site_caches(ctx);
   cudaFree(ctx->dw_coef);
-  cudaFree(ctx->clover.f);
-  cudaFree(ctx->clover.h);
-  cudaFree(ctx->clover.ht);
-  cudaFree(ctx->clover_inv.d);
-  cudaFree(ctx->clover_inv.f);
-  cudaFree(ctx->clover_inv.h);
-  cudaFree(ctx->clover_inv.ht);
   cudaFree(ctx->partials);
   cudaFree(ctx->counter);
   cudaFree(ctx->st_dev);
@@ -331,6 +344,10 @@ int lmb_set_geometry(lmb_ctx *ctx, const int L[4], int nw, const double phase_re
   if (changed) {
     for (auto &ls : ctx->links) ls.valid = false;
     ctx->smear.valid = false;
+  }
+  if (V != ctx->cache_V) {  // caches built for another volume
+    release_site_caches(ctx);
+    ctx->cache_V = V;
   }
   return LMB_OK;
 }
@@ -453,6 +470,28 @@ int lmb_cg_ddagd(lmb_ctx *ctx, const lmb_cg_params *prm, void *x, const void *b,
       return cg_dispatch(ctx, prm, StaggeredPolicy{true, prm->mass, prm->naik_epsilon}, x, b, res, st);
     case LMB_OP_DOMAINWALL:
       return cg_dispatch(ctx, prm, DWPolicy{}, x, b, res, st);
+    default: return fail(ctx, LMB_ERR_ARG, "unknown operator %d", prm->op);
+  }
+}
+
+int lmb_operator_timing(lmb_ctx *ctx, const lmb_cg_params *prm, const void *in, int napply, int dagger,
+                        double *ms_per_apply, void *stream) {
+  if (!ctx_ok(ctx)) return LMB_ERR_ARG;
+  if (!prm || !in || !ms_per_apply) return fail(ctx, LMB_ERR_ARG, "null argument");
+  const int prec = prm->precision;
+  switch (prm->op) {
+    case LMB_OP_WILSON:
+    case LMB_OP_WILSON_CLOVER:
+      return time_dispatch(ctx, WilsonPolicy{prm->op, prm->kappa, prm->csw}, in, napply, dagger, prec, ms_per_apply,
+                           stream);
+    case LMB_OP_STAGGERED:
+      return time_dispatch(ctx, StaggeredPolicy{false, prm->mass, 0.0}, in, napply, dagger, prec, ms_per_apply,
+                           stream);
+    case LMB_OP_HISQ:
+      return time_dispatch(ctx, StaggeredPolicy{true, prm->mass, prm->naik_epsilon}, in, napply, dagger, prec,
+                           ms_per_apply, stream);
+    case LMB_OP_DOMAINWALL:
+      return time_dispatch(ctx, DWPolicy{}, in, napply, dagger, prec, ms_per_apply, stream);
     default: return fail(ctx, LMB_ERR_ARG, "unknown operator %d", prm->op);
   }
 }

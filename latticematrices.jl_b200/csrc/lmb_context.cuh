@@ -109,6 +109,7 @@ struct lmb_ctx {
   bool dw_two_pass = false;
   lmb::CloverCache clover;
   lmb::CloverCache clover_inv;  // A^-1 blocks (even/odd solve)
+  int64_t cache_V = 0;          // volume the link sets and clover caches are sized for
   // parity-ordered copies of link / clover storage for the even/odd solve:
   // workspace name -> (source version, volume, buffer) they were built for
   struct EoTag {

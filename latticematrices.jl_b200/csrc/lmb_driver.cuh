@@ -37,6 +37,57 @@ int apply_generic(lmb_ctx *ctx, const Op &op, void *out, const void *in, int dag
   return op_unpack_out(ctx, op, out, fout, st);
 }
 
+// device time per application of the operator between two resident
+// internal fields, input and output swapped after every application (the
+// protocol of benchmark/HISQ_DIRAC_BENCHMARK_2026-08-17.md:10-31); two
+// untimed applications first
+template <int PS, class Op>
+int time_generic(lmb_ctx *ctx, const Op &op, const void *in, int napply, int dagger, double *ms, cudaStream_t st) {
+  constexpr int NC = Op::NC;
+  const int64_t V = op_volume(ctx, op);
+  Field<PS, NC> f[2];
+  if (!make_field(ctx, "apply_in", f[0], V) || !make_field(ctx, "apply_out", f[1], V))
+    return fail(ctx, LMB_ERR_CUDA, "out of device memory (apply workspaces)");
+  int rc = op_pack_in(ctx, op, f[0], in, st);
+  if (rc) return rc;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    if (e0) cudaEventDestroy(e0);
+    return fail(ctx, LMB_ERR_CUDA, "event creation failed");
+  }
+  for (int i = 0; i < napply + 2 && rc == LMB_OK; i++) {
+    if (i == 2) cudaEventRecord(e0, st);
+    EpiStore<PS, NC> epi{f[(i + 1) & 1], nullptr};
+    rc = dagger ? op.template launch<PS, 1>(ctx, f[i & 1], epi, st) : op.template launch<PS, 0>(ctx, f[i & 1], epi, st);
+  }
+  cudaEventRecord(e1, st);
+  float t = 0.f;
+  const cudaError_t e = cudaEventSynchronize(e1);
+  if (e == cudaSuccess) cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  if (e != cudaSuccess) return fail(ctx, LMB_ERR_CUDA, "%s", cudaGetErrorString(e));
+  *ms = napply > 0 ? (double)t / napply : 0.0;
+  return LMB_OK;
+}
+
+template <class Op>
+int time_dispatch(lmb_ctx *ctx, const Op &op, const void *in, int napply, int dagger, int prec, double *ms,
+                  void *stream) {
+  if (!ctx_ok(ctx)) return LMB_ERR_ARG;
+  if (!in || !ms) return fail(ctx, LMB_ERR_ARG, "null argument");
+  if (napply < 1) return fail(ctx, LMB_ERR_ARG, "napply must be positive");
+  cudaStream_t st = as_stream(stream);
+  int rc = op.prepare(ctx, prec, st);
+  if (rc) return rc;
+  switch (prec) {
+    case PREC_DOUBLE: return time_generic<PREC_DOUBLE>(ctx, op, in, napply, dagger, ms, st);
+    case PREC_SINGLE: return time_generic<PREC_SINGLE>(ctx, op, in, napply, dagger, ms, st);
+    default: return time_generic<PREC_HALF>(ctx, op, in, napply, dagger, ms, st);
+  }
+}
+
 template <class Op>
 int apply_dispatch(lmb_ctx *ctx, const Op &op, void *out, const void *in, int dagger, int prec, void *stream) {
   if (!ctx_ok(ctx)) return LMB_ERR_ARG;
@@ -296,6 +347,8 @@ int cg_dispatch(lmb_ctx *ctx, const lmb_cg_params *prm, const Op &op, void *x, c
 // declares them, empty defines them
 #define LMB_OP_INSTANCE(EXT, OP, PS, PX)                                                                  \
   EXT template int apply_generic<PS, OP>(lmb_ctx *, const OP &, void *, const void *, int, cudaStream_t); \
+  EXT template int time_generic<PS, OP>(lmb_ctx *, const OP &, const void *, int, int, double *,         \
+                                        cudaStream_t);                                                   \
   EXT template int cg_run<PS, PX, OP>(lmb_ctx *, const lmb_cg_params *, const OP &, void *, const void *, \
                                       lmb_cg_result *, cudaStream_t);
 #define LMB_OP_INSTANCES(EXT, OP)                    \

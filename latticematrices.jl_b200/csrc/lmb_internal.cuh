@@ -45,6 +45,7 @@ int read_state(lmb_ctx *ctx, cudaStream_t st);
 int pack_links_to(lmb_ctx *ctx, double2 *dst, const void *const U[4], cudaStream_t st);
 int unpack_links_from(lmb_ctx *ctx, void *const U[4], const double2 *src, cudaStream_t st);
 int check_links_arg(lmb_ctx *ctx, const void *const U[4], const char *what);
+void release_site_caches(lmb_ctx *ctx);
 // even/odd caches (lmb_schur_ops.cu)
 int ensure_clover_inverse(lmb_ctx *ctx, int prec, cudaStream_t st);
 int ensure_eo_copies(lmb_ctx *ctx, int prec, bool clover, cudaStream_t st);

@@ -25,4 +25,4 @@ from .domainwall import (D5DW_GeneralizedDomainwallOperator5D,  # noqa: F401
                          D5DW_MobiusDomainwallOperator5D)
 from .inputs import gaussian_fermion, random_su3_links  # noqa: F401
 from .solver import (CGResult, DdagDOp, cg_, cg_batched_, dot,  # noqa: F401
-                     pseudofermion_action, solve_, solve_evenodd_)
+                     operator_timing, pseudofermion_action, solve_, solve_evenodd_)

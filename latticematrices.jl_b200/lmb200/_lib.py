@@ -39,7 +39,7 @@ EXPORTED = (
     "lmb_hisq_link_pullback", "lmb_hisq_fermion_force",
     "lmb_wilson_clover_link_pullback", "lmb_wilson_clover_fermion_force",
     "lmb_domainwall_set", "lmb_domainwall_apply", "lmb_solve_evenodd",
-    "lmb_set_halo",
+    "lmb_set_halo", "lmb_operator_timing",
 )
 
 
@@ -176,6 +176,8 @@ def load(path: str = LIB_PATH):
         lib.lmb_solve_evenodd.argtypes = [vp, ctypes.POINTER(CGParams), vp,
                                           vp, ctypes.POINTER(CGResultC), vp]
         lib.lmb_field_dot.argtypes = [vp, vp, vp, ctypes.c_int, dp, vp]
+        lib.lmb_operator_timing.argtypes = [vp, ctypes.POINTER(CGParams), vp,
+                                            ctypes.c_int, ctypes.c_int, dp, vp]
         lib.lmb_random_su3_links.argtypes = [vp, ctypes.POINTER(vp),
                                              ctypes.c_double, ctypes.c_uint64,
                                              vp]

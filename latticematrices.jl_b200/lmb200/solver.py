@@ -159,6 +159,37 @@ def cg_(x, A, b, r=None, p=None, Ap=None, *, rtol=1e-10, atol=0.0,
     return _cg_generic(x, A, b, r, p, Ap, rtol, atol, maxiter)
 
 
+def operator_timing(D, psi, napply=50, *, precision="double", dagger=False):
+    """Device milliseconds per application of D (or D^+) on the library's
+    resident fields (lmb_operator_timing): psi is packed once, then D is
+    applied 2 + napply times with input and output swapped after each
+    application, the last napply timed with CUDA events.  The loop of
+    benchmark/hisq_dirac_scaling.jl:82-100 without its per-call layout: what
+    one Krylov iteration pays for the stencil."""
+    if precision not in PREC:
+        raise ArgumentError(f"unknown precision {precision!r}")
+    native = _native_operator(DdagDOp(D, psi))
+    if native is None:
+        raise ArgumentError("operator_timing needs a native Dirac operator")
+    require_single_rank(psi)
+    D, op = native
+    binder = D.wilson if op == OP_WILSON_CLOVER else D
+    prm = CGParams()
+    prm.op = op
+    prm.kappa = getattr(D, "kappa", 0.0)
+    prm.csw = getattr(D, "cSW", 0.0)
+    prm.mass = getattr(D, "mass", 0.0)
+    prm.naik_epsilon = getattr(D, "naik_epsilon", 0.0)
+    prm.precision = PREC[precision]
+    st = _stream()
+    ctx = binder._bind(psi, st)
+    ms = ctypes.c_double()
+    ctx.check(ctx.lib.lmb_operator_timing(ctx.handle, ctypes.byref(prm),
+                                          psi.data_ptr(), int(napply),
+                                          int(bool(dagger)), ctypes.byref(ms), st))
+    return ms.value
+
+
 def solve_evenodd_(x, D, b, *, rtol=1e-10, atol=0.0, maxiter=5000,
                    precision="double", delta=0.1, check_interval=0,
                    profile=False):

@@ -99,3 +99,18 @@ def test_cached_hisq_operator_follows_links(lmb, orc):
     X2, L2 = orc.hisq_links_from_thin(U2, -0.083)
     ref2 = orc.hisq(X2, L2, psi, 0.05, -0.083, PHASES, dagger=True)
     assert rd.rel_err(out.gather_matrix(), ref2) <= 1e-12
+
+
+def test_shared_context_follows_a_growing_lattice(lmb, orc):
+    """The smearing context is shared by every field of a device; its link
+    and clover caches are sized by the volume, so a larger lattice after a
+    smaller one must rebuild them (regression: a 16^4 smearing after 8^4
+    copied into the 8^4-sized link set)."""
+    for L in ((4, 4, 4, 4), (6, 4, 6, 8), (4, 4, 4, 4)):
+        U = orc.random_su3_links(L, 0.25, 5)
+        Ud = [lmb.LatticeMatrix.from_array(u, nw=3) for u in U]
+        links = lmb.hisq_links_from_thin(Ud, -0.083)
+        X, Ln = orc.hisq_links_from_thin(U, -0.083)
+        for mu in range(4):
+            assert rd.rel_err(links.fat_links[mu].gather_matrix(), X[mu]) <= 1e-12
+            assert rd.rel_err(links.long_links[mu].gather_matrix(), Ln[mu]) <= 1e-12

@@ -167,3 +167,19 @@ def test_staggered_validation(lmb, orc):
         lmb.mul_(bad.similar(), D, bad)
     with pytest.raises(lmb.ArgumentError, match="finite"):
         lmb.StaggeredDiracOperator4D(Ud, float("nan"))
+
+
+def test_operator_timing_on_resident_fields(lmb, orc):
+    """lmb_operator_timing: device time per application of the bound
+    operator on the library's internal fields (the bench's Dslash rate)."""
+    L = (8, 8, 8, 8)
+    U = lmb.random_su3_links(L, 0.25, 1, nw=3)
+    links = lmb.hisq_links_from_thin(U, -0.083)
+    D = lmb.HISQDiracOperator4D(links, 0.0, -0.083)
+    psi = lmb.gaussian_fermion(L, 3, 1, 2, nw=3, phases=PHASES)
+    for prec in ("double", "single", "half"):
+        ms = lmb.operator_timing(D, psi, 5, precision=prec)
+        assert 0.0 < ms < 100.0, (prec, ms)
+    assert lmb.operator_timing(D, psi, 3, dagger=True) > 0.0
+    with pytest.raises(lmb.ArgumentError):
+        lmb.operator_timing(D, psi, 0)
