@@ -107,6 +107,10 @@ def parse():
                          "D'D CG route; hisq_dslash: one FP64 HISQ D application "
                          "at 8^4 .. 32^4 beside the reference's published table")
     ap.add_argument("--l5", type=int, default=12)
+    ap.add_argument("--hisq-sizes", default="8,16,24,32",
+                    help="hisq_dslash: lattice extents L of the L^4 lattices")
+    ap.add_argument("--samples", type=int, default=9,
+                    help="hisq_dslash: timing samples per size")
     ap.add_argument("--fd-directions", type=int, default=64)
     return ap.parse_args()
 
@@ -597,7 +601,7 @@ def run_hisq_dslash(args):
     peak, peak_kind = measured_peak()
     st = torch.cuda.current_stream()
     rows = []
-    for n in (8, 16, 24, 32):
+    for n in (int(v) for v in args.hisq_sizes.split(",")):
         L = (n, n, n, n)
         sites = n ** 4
         U = lmb.random_su3_links(L, 0.25, 1, nw=3)
@@ -608,7 +612,7 @@ def run_hisq_dslash(args):
         napply = max(20, min(2000, int(2e8 // sites)))
         row = {"L": n, "sites": sites, "napply_per_sample": napply}
         for prec, rb in (("double", 8), ("single", 4)):
-            samples = [lmb.operator_timing(D, psi, napply, precision=prec) for _ in range(9)]
+            samples = [lmb.operator_timing(D, psi, napply, precision=prec) for _ in range(args.samples)]
             ms = statistics.median(samples)
             gbs = 156 * rb * sites / (ms * 1e-3) / 1e9
             row[prec] = {"resident_ms_median": ms, "resident_ms_min": min(samples),
@@ -619,7 +623,7 @@ def run_hisq_dslash(args):
             lmb.mul_(b, D, a)
             a, b = b, a
         samples = []
-        for _ in range(9):
+        for _ in range(args.samples):
             k = max(5, napply // 4)
             def loop():
                 nonlocal a, b
@@ -629,9 +633,10 @@ def run_hisq_dslash(args):
             _, sec = _timed(loop, st)
             samples.append(sec * 1e3 / k)
         row["double"]["api_ms_median"] = statistics.median(samples)
-        lm, sq = HISQ_PUBLISHED_MS[n]
-        row["published_h100_ms"] = {"latticematrices_median": lm, "simulateqcd_median": sq}
-        row["speedup_vs_latticematrices_h100"] = lm / row["double"]["resident_ms_median"]
+        if n in HISQ_PUBLISHED_MS:
+            lm, sq = HISQ_PUBLISHED_MS[n]
+            row["published_h100_ms"] = {"latticematrices_median": lm, "simulateqcd_median": sq}
+            row["speedup_vs_latticematrices_h100"] = lm / row["double"]["resident_ms_median"]
         rows.append(row)
         del U, links, D, psi, out, a, b
         torch.cuda.empty_cache()

@@ -49,6 +49,14 @@ struct StaggeredPolicy {
     if (naik) {
       const Gauge<P> X = gauge_view<P>(ctx->links[LMB_LINKS_FAT], g.V);
       const Gauge<P> Lk = gauge_view<P>(ctx->links[LMB_LINKS_LONG], g.V);
+      if constexpr (PersistentEpi<Epi>::value && P == PREC_DOUBLE) {
+        if (ctx->persistent) {
+          auto kern = staggered_persistent_kernel<R, true, PHM, Field<P, 3>, Gauge<P>, Gauge<P>, Epi>;
+          const unsigned g2 = std::min(grid, resident_grid(ctx, kern));
+          kern<<<g2, kStagThreads, 0, st>>>(g, in, X, Lk, (R)mass, fc, lc, epi, (int)grid);
+          return;
+        }
+      }
       staggered_dslash_kernel<R, true, PHM><<<grid, kStagThreads, 0, st>>>(g, in, X, Lk, (R)mass, fc, lc, epi);
     } else {
       const LinkSet &ls = ctx->links[LMB_LINKS_THIN];

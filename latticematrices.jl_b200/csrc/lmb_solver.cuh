@@ -156,6 +156,12 @@ struct EpiStoreNorm {  // K1
     finish(n2);
   }
   // persistent kernels: store and add |v|^2 to red; finish() once per block
+  template <typename R> LMB_D void site_acc(int s, bool active, const Cx<R> *v, double (&red)[1]) const {
+    if (active) {
+      out.store(s, v);
+      red[0] += sum_norm2(v, NC);
+    }
+  }
   LMB_D void pair_adj_acc(int s0, bool active, const Cx2 *v, double (&red)[1]) const {
     if (active) {
       store_adj(out, s0, v);

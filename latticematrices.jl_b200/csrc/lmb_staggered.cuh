@@ -16,6 +16,17 @@
 namespace lmb {
 
 constexpr int kStagThreads = kDslashThreads;  // the epilogue reductions assume it
+// minimum resident blocks per SM requested for the one-site stencil and its
+// persistent form
+#ifndef LMB_STAG_MINB
+#define LMB_STAG_MINB 0
+#endif
+#ifndef LMB_STAG_PMINB
+#define LMB_STAG_PMINB 4
+#endif
+#ifndef LMB_STAG_K2MINB
+#define LMB_STAG_K2MINB 4
+#endif
 
 // neighbour at signed distance d along mu with the number of edge crossings
 // (the loops run at most once on extents >= 3; measured faster on B200 than
@@ -125,41 +136,81 @@ struct NoLinks {
   template <typename R> LMB_D void load(int, int64_t, Cx<R> *) const {}
 };
 
+// D psi at site s (3 components)
+template <typename R, bool NAIK, int PHM, class SF, class GF, class GL>
+LMB_D void stag_site(const Geom &g, int s, const SF &in, const GF &X, const GL &Lk, R mass, R fc, R lc,
+                     Cx<R> *out) {
+  int c[4];
+  site_coords(g, s, c);
+  const int p0 = c[0] + g.eta_off[0], p1 = p0 + c[1] + g.eta_off[1], p2 = p1 + c[2] + g.eta_off[2];
+  const R eta[4] = {(R)1, (p0 & 1) ? (R)-1 : (R)1, (p1 & 1) ? (R)-1 : (R)1, (p2 & 1) ? (R)-1 : (R)1};
+  Cx<R> fat[3] = {Cx<R>(0, 0), Cx<R>(0, 0), Cx<R>(0, 0)};
+  stag_hop<R, 0, 1, PHM>(g, s, c, in, X, eta[0], fat);
+  stag_hop<R, 1, 1, PHM>(g, s, c, in, X, eta[1], fat);
+  stag_hop<R, 2, 1, PHM>(g, s, c, in, X, eta[2], fat);
+  stag_hop<R, 3, 1, PHM>(g, s, c, in, X, eta[3], fat);
+  Cx<R> psi[3];
+  in.load(s, psi);
+  if constexpr (NAIK) {
+    Cx<R> lng[3] = {Cx<R>(0, 0), Cx<R>(0, 0), Cx<R>(0, 0)};
+    stag_hop<R, 0, 3, PHM>(g, s, c, in, Lk, eta[0], lng);
+    stag_hop<R, 1, 3, PHM>(g, s, c, in, Lk, eta[1], lng);
+    stag_hop<R, 2, 3, PHM>(g, s, c, in, Lk, eta[2], lng);
+    stag_hop<R, 3, 3, PHM>(g, s, c, in, Lk, eta[3], lng);
+#pragma unroll
+    for (int i = 0; i < 3; i++) out[i] = mass * psi[i] + fc * fat[i] + lc * lng[i];
+  } else {
+#pragma unroll
+    for (int i = 0; i < 3; i++) out[i] = mass * psi[i] + fc * fat[i];
+  }
+}
+
+template <int PS, int NC> struct EpiStore;  // lmb_solver.cuh
+template <int PS, int PX, int NC> struct EpiCGUpdate;
+
+// resident blocks per SM requested from the register allocator: the plain
+// FP64 store (mul!, the Dslash rate) is latency bound at 104 registers and
+// runs ~11 % faster with five 128-thread blocks per SM (96 registers); the
+// CG epilogues spill at that bound and keep the default, except the
+// persistent K1 and the K2 update, whose four blocks per SM (128
+// registers, a few words spilled) measured faster than three (48^3x96 FP64
+// HISQ: K1 3.42 against 3.60 ms, K2 3.87 against 4.34 ms)
+template <typename R, class Epi> struct StagMinBlocks { static constexpr int value = LMB_STAG_MINB; };
+template <int NC> struct StagMinBlocks<double, EpiStore<PREC_DOUBLE, NC>> { static constexpr int value = 5; };
+template <int NC> struct StagMinBlocks<double, EpiCGUpdate<PREC_DOUBLE, PREC_DOUBLE, NC>> {
+  static constexpr int value = LMB_STAG_K2MINB;
+};
+
 // Epi as for the Wilson kernel, on 3-component fields
 template <typename R, bool NAIK, int PHM, class SF, class GF, class GL, class Epi>
-__global__ void __launch_bounds__(kStagThreads)
+__global__ void __launch_bounds__(kStagThreads, (StagMinBlocks<R, Epi>::value))
     staggered_dslash_kernel(const Geom g, const SF in, const GF X, const GL Lk, const R mass, const R fc,
                             const R lc, Epi epi) {
   if (epi.skip()) return;
   const int s = blockIdx.x * kStagThreads + threadIdx.x;
   const bool active = s < g.V;
   Cx<R> out[3];
-  if (active) {
-    int c[4];
-    site_coords(g, s, c);
-    const int p0 = c[0] + g.eta_off[0], p1 = p0 + c[1] + g.eta_off[1], p2 = p1 + c[2] + g.eta_off[2];
-    const R eta[4] = {(R)1, (p0 & 1) ? (R)-1 : (R)1, (p1 & 1) ? (R)-1 : (R)1, (p2 & 1) ? (R)-1 : (R)1};
-    Cx<R> fat[3] = {Cx<R>(0, 0), Cx<R>(0, 0), Cx<R>(0, 0)};
-    stag_hop<R, 0, 1, PHM>(g, s, c, in, X, eta[0], fat);
-    stag_hop<R, 1, 1, PHM>(g, s, c, in, X, eta[1], fat);
-    stag_hop<R, 2, 1, PHM>(g, s, c, in, X, eta[2], fat);
-    stag_hop<R, 3, 1, PHM>(g, s, c, in, X, eta[3], fat);
-    Cx<R> psi[3];
-    in.load(s, psi);
-    if constexpr (NAIK) {
-      Cx<R> lng[3] = {Cx<R>(0, 0), Cx<R>(0, 0), Cx<R>(0, 0)};
-      stag_hop<R, 0, 3, PHM>(g, s, c, in, Lk, eta[0], lng);
-      stag_hop<R, 1, 3, PHM>(g, s, c, in, Lk, eta[1], lng);
-      stag_hop<R, 2, 3, PHM>(g, s, c, in, Lk, eta[2], lng);
-      stag_hop<R, 3, 3, PHM>(g, s, c, in, Lk, eta[3], lng);
-#pragma unroll
-      for (int i = 0; i < 3; i++) out[i] = mass * psi[i] + fc * fat[i] + lc * lng[i];
-    } else {
-#pragma unroll
-      for (int i = 0; i < 3; i++) out[i] = mass * psi[i] + fc * fat[i];
-    }
-  }
+  if (active) stag_site<R, NAIK, PHM>(g, s, in, X, Lk, mass, fc, lc, out);
   epi(s, active, out);
+}
+
+// Persistent form for the reducing CG epilogues (see
+// wilson_half_adj_persistent_kernel): the resident blocks walk the tiles in a
+// fixed order, the reduction is carried in registers and done once per block
+template <typename R, bool NAIK, int PHM, class SF, class GF, class GL, class Epi>
+__global__ void __launch_bounds__(kStagThreads, LMB_STAG_PMINB)
+    staggered_persistent_kernel(const Geom g, const SF in, const GF X, const GL Lk, const R mass, const R fc,
+                                const R lc, Epi epi, int ntiles) {
+  if (epi.skip()) return;
+  double red[1] = {0.0};
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int s = tile * kStagThreads + threadIdx.x;
+    const bool active = s < g.V;
+    Cx<R> out[3];
+    if (active) stag_site<R, NAIK, PHM>(g, s, in, X, Lk, mass, fc, lc, out);
+    epi.site_acc(s, active, out, red);
+  }
+  epi.finish(red);
 }
 
 // ---------------------------------------------------------------------------
