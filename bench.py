@@ -36,8 +36,9 @@ PHASES = (1, 1, 1, -1)
 
 # Plain FP64 CG iterations this workload needs (32^3x64, kappa 0.1355,
 # cSW 1.0, links exp(0.2 i H) seed 1, source seed 2, rtol 1e-10), measured by
-# the GPU FP64 solve of this file; the CPU reference arm multiplies its
-# per-iteration time by it.
+# the GPU FP64 solve of this file and by a complete oracle solve; the CPU
+# reference arm multiplies its per-iteration time by the count of its own
+# complete solve, or by this constant with --no-full-solve or under torchrun.
 FP64_ITERATIONS_32x64 = 450
 
 # Algorithmic bytes per lattice site of the two stencil kernels of a CG
@@ -93,6 +94,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
+    ap.add_argument("--no-full-solve", action="store_true",
+                    help="reference arm: skip the complete FP64 oracle solve that fixes the "
+                         "iteration count (about two minutes on 16 cores at 32^3x64)")
     ap.add_argument("--workload", default="clover",
                     choices=["clover", "wilson8", "hisq", "hisq_dslash", "batched", "force",
                              "clover_force", "dw", "evenodd"],
@@ -265,12 +269,25 @@ def run_reference(args):
         per.append(orc.cg_iterations_seconds(op, b, 1))
     t_iter = statistics.mean(per)
     iters = FP64_ITERATIONS_32x64 if L == (32, 32, 32, 64) else None
+    full = None
+    if ws == 1 and not args.no_full_solve:
+        # one complete FP64 solve to the workload's tolerance (not in the
+        # per-iteration sample): its iteration count replaces the constant
+        import numpy as np
+        t0 = time.perf_counter()
+        xs, res = orc.cg_ddagd(op, b, rtol=args.rtol, maxiter=args.maxiter)
+        t_full = time.perf_counter() - t0
+        true_rel = float(np.linalg.norm(b - op.ddagd(xs)) / np.linalg.norm(b))
+        full = {"iterations": res["iterations"], "converged": res["converged"],
+                "time_s": t_full, "true_rel_residual": true_rel}
+        iters = res["iterations"]
     value = t_iter * iters if iters else t_iter
     unit = "s" if iters else "s/iteration"
     sample = (f"{args.steps} FP64 CG iterations (D'D clover + BLAS) on the "
               f"full {L} lattice after {args.warmup} warm-up iterations; "
               f"value = mean seconds per iteration x {iters} iterations "
-              f"(the FP64 iteration count of this workload)"
+              + ("(the iteration count of the complete FP64 solve run here)" if full else
+                 "(the FP64 iteration count of this workload)")
               if iters else "seconds per FP64 CG iteration")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": unit,
@@ -286,6 +303,8 @@ def run_reference(args):
         "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    if full:
+        line["full_solve"] = full
     print(json.dumps(line), flush=True)
 
 
@@ -384,6 +403,26 @@ def run_lmb(args):
     t_e2e = max_over_ranks(start.elapsed_time(end) / 1e3 / args.steps, ws, dev)
     nbytes = b_host.numel() * b_host.element_size()
 
+    # ---- per-configuration setup (a new gauge field): link repack, SU(3)
+    # check + reconstruct-12 copies, F_mu_nu, clover blocks, their FP32 /
+    # int16 copies -- what update_clover! rebuilds per gauge update
+    # (WilsonDiracCloverOperator.jl:392-399, 468-479).  Timed as a
+    # zero-iteration solve right after the links' epochs change, minus the
+    # same call with warm caches.
+    def zero_solve():
+        lmb.clear_matrix_(x)
+        return lmb.cg_(x, A, b, rtol=args.rtol, maxiter=0, precision=prec, delta=args.delta)
+
+    zero_solve()
+    setup_samples = []
+    for _ in range(3):
+        _, warm = _timed(zero_solve, stream)
+        for u in U:
+            lmb.mark_halo_dirty_(u)
+        _, cold = _timed(zero_solve, stream)
+        setup_samples.append(cold - warm)
+    setup_ms = statistics.median(setup_samples) * 1e3
+
     # ---- roofline of the dominant stencil kernel (mixed solve) ----
     k1_ms = sum(r.dslash_ms for r in results)
     k2_ms = sum(r.update_ms for r in results)
@@ -447,7 +486,10 @@ def run_lmb(args):
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": achieved / peak,
                      "bytes_per_site": bps,
-                     "traffic": traffic * sites if traffic else None},
+                     "traffic": traffic * sites if traffic else None,
+                     "k1_frac": k1_gbs / peak, "k2_frac": k2_gbs / peak,
+                     "fp64_k1_frac": gbs64 / peak, "fp64_k2_frac": gbs64_k2 / peak},
+        "setup_ms": setup_ms,
         "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": nbytes,
                 "d2h_bytes_per_step": nbytes},
         "gpu_launches": int(sum(r.kernel_launches for r in results)),
