@@ -113,6 +113,8 @@ def parse():
     ap.add_argument("--l5", type=int, default=12)
     ap.add_argument("--hisq-sizes", default="8,16,24,32",
                     help="hisq_dslash: lattice extents L of the L^4 lattices")
+    ap.add_argument("--batched-small", action="store_true",
+                    help="batched: 16^4 x8 + 8^4 x4 instead of the benchmark set (profiling)")
     ap.add_argument("--samples", type=int, default=9,
                     help="hisq_dslash: timing samples per size")
     ap.add_argument("--fd-directions", type=int, default=64)
@@ -696,6 +698,8 @@ def run_batched(args):
     import lmb200 as lmb
     shapes = [((32, 32, 32, 32), 16), ((8, 8, 8, 8), 4), ((12, 12, 12, 12), 4),
               ((16, 16, 16, 16), 2), ((24, 24, 24, 24), 1)]
+    if args.batched_small:       # a small case of the same kernels (profiling)
+        shapes = [((16, 16, 16, 16), 8), ((8, 8, 8, 8), 4)]
     systems = []
     for i, (L, n) in enumerate(shapes):
         U = lmb.random_su3_links(L, 0.2, 10 + i)
@@ -729,7 +733,8 @@ def run_batched(args):
     clear()
     rs, t_seq = _timed(sequential, st)
     total_sites_rhs = sum(L[0] * L[1] * L[2] * L[3] * n for L, n in shapes)
-    print(json.dumps({"workload": "batched Wilson D'D CG: 32^4 x16 + 8^4 x4 + 12^4 x4 + 16^4 x2 + 24^4 x1",
+    print(json.dumps({"workload": "batched Wilson D'D CG: " + " + ".join(
+                          "%d^4 x%d" % (L[0], n) for L, n in shapes),
                       "batched_s": t_batch, "sequential_s": t_seq, "speedup": t_seq / t_batch,
                       "all_converged": all(r.converged for r in res),
                       "max_iterations": max(r.iterations for r in res),

@@ -181,43 +181,34 @@ __global__ void __launch_bounds__(kSmearThreads)
 }
 
 // U(3) projection pullback (HISQPullback.jl:319-424): with W = V H^{-1},
-// H = (V^+V)^{1/2}, solve H X + X H = W^+ dW - dW^+ W (a 9x9 linear system,
-// LU with partial pivoting) and accumulate dV += W X.
-LMB_D void solve9(Cx<double> (*A)[9], Cx<double> *b) {
-  for (int k = 0; k < 9; k++) {
-    int piv = k;
-    double best = norm2(A[k][k]);
-    for (int r = k + 1; r < 9; r++) {
-      const double v = norm2(A[r][k]);
-      if (v > best) {
-        best = v;
-        piv = r;
-      }
+// H = (V^+V)^{1/2}, the cotangent is dV = W X where X solves the Sylvester
+// equation H X + X H = C, C = W^+ dW - dW^+ W.  The reference solves it as a
+// 9x9 linear system; here it is solved in closed form from the Cayley-
+// Hamilton theorem.  For A X - X B = C, sum_k a_k (A^k X - X B^k) =
+// sum_k a_k sum_{j<k} A^j C B^{k-1-j}, and with a_k the coefficients of the
+// characteristic polynomial of B the X B^k terms cancel.  Taking A = H,
+// B = -H: det(z + H) = z^3 + u z^2 + v z + w (u, v, w the elementary
+// symmetric functions of the eigenvalues sqrt(g_i) of H, from the
+// projection), so
+//   M X = v C + u (H C - C H) + H^2 C - H C H + C H^2,
+//   M = H^3 + u H^2 + v H + w,
+// M Hermitian positive definite (eigenvalues (h_i + h_j)(h_i + h_k) 2 h_i,
+// no differences of eigenvalues), inverted by its adjugate.  Everything
+// stays in registers (the 9x9 system took a 1.5 KB local-memory frame).
+LMB_D void mat3_inverse(const Cx<double> *m, Cx<double> *inv) {
+  // column-major m[r + 3c]; inv = adj(m) / det(m)
+  auto at = [&](int r, int c) { return m[r + 3 * c]; };
+  Cx<double> cof[9];
+  for (int r = 0; r < 3; r++)
+    for (int c = 0; c < 3; c++) {
+      const int r1 = (r + 1) % 3, r2 = (r + 2) % 3, c1 = (c + 1) % 3, c2 = (c + 2) % 3;
+      cof[r + 3 * c] = at(r1, c1) * at(r2, c2) - at(r1, c2) * at(r2, c1);
     }
-    if (piv != k) {
-      for (int c = 0; c < 9; c++) {
-        const Cx<double> t = A[k][c];
-        A[k][c] = A[piv][c];
-        A[piv][c] = t;
-      }
-      const Cx<double> t = b[k];
-      b[k] = b[piv];
-      b[piv] = t;
-    }
-    const double d = norm2(A[k][k]);
-    const Cx<double> inv = d > 0 ? Cx<double>(A[k][k].re / d, -A[k][k].im / d) : Cx<double>(0, 0);
-    for (int r = k + 1; r < 9; r++) {
-      const Cx<double> f = A[r][k] * inv;
-      for (int c = k; c < 9; c++) A[r][c] = A[r][c] - f * A[k][c];
-      b[r] = b[r] - f * b[k];
-    }
-  }
-  for (int r = 8; r >= 0; r--) {
-    Cx<double> v = b[r];
-    for (int c = r + 1; c < 9; c++) v = v - A[r][c] * b[c];
-    const double d = norm2(A[r][r]);
-    b[r] = d > 0 ? v * Cx<double>(A[r][r].re / d, -A[r][r].im / d) : Cx<double>(0, 0);
-  }
+  Cx<double> det = at(0, 0) * cof[0] + at(0, 1) * cof[3] + at(0, 2) * cof[6];
+  const double dn = norm2(det);
+  const Cx<double> idet = dn > 0 ? Cx<double>(det.re / dn, -det.im / dn) : Cx<double>(0, 0);
+  for (int r = 0; r < 3; r++)
+    for (int c = 0; c < 3; c++) inv[r + 3 * c] = cof[c + 3 * r] * idet;  // transpose of the cofactors
 }
 
 template <int = 0>
@@ -227,71 +218,55 @@ __global__ void __launch_bounds__(64)
   if (t >= 4 * n) return;
   const int mu = (int)(t / n);
   const int s = (int)(t - (int64_t)mu * n);
-  Cx<double> Vm[9], W[9], dWm[9], Q[9], Q2[9], inv[9], H[9];
+  Cx<double> Vm[9], W[9], H[9], C[9];
   load9(Vall + (size_t)mu * 9 * n, n, s, Vm);
-  load9(dW + (size_t)mu * 9 * n, n, s, dWm);
-  // W and H from the projection formulas
-  mat3_adj_mul(Vm, Vm, Q);
-  mat3_mul(Q, Q, Q2);
+  double u, v, w;
   {
-    double c0 = 0, trQ2 = 0, trQ3 = 0;
-    for (int i = 0; i < 3; i++) {
-      c0 += Q[i + 3 * i].re;
-      trQ2 += Q2[i + 3 * i].re;
-      for (int j = 0; j < 3; j++) trQ3 += (Q2[i + 3 * j] * Q[j + 3 * i]).re;
-    }
-    const double c1 = trQ2 / 2, c2 = trQ3 / 3;
-    double S = c1 / 3 - c0 * c0 / 18;
-    double g0, g1, g2;
-    if (fabs(S) < 1e-7) {
-      g0 = g1 = g2 = c0 / 3;
-    } else {
-      S = sqrt(fmax(S, 0.0));
-      const double R = c2 / 2 - c0 * c1 / 3 + c0 * c0 * c0 / 27;
-      double ratio = fmin(1.0, fmax(-1.0, R / (S * S * S)));
-      const double theta = acos(ratio);
-      const double tpt = 2.0943951023931954923;
-      g0 = c0 / 3 + 2 * S * cos(theta / 3 - tpt);
-      g1 = c0 / 3 + 2 * S * cos(theta / 3);
-      g2 = c0 / 3 + 2 * S * cos(theta / 3 + tpt);
-    }
-    const double fl = 2.220446049250313e-16;
-    g0 = fmax(g0, fl);
-    g1 = fmax(g1, fl);
-    g2 = fmax(g2, fl);
-    const double u = sqrt(g0) + sqrt(g1) + sqrt(g2);
-    const double v = sqrt(g0 * g1) + sqrt(g0 * g2) + sqrt(g1 * g2);
-    const double w = sqrt(g0 * g1 * g2);
-    const double den = w * (u * v - w);
-    const double f0 = (-w * (u * u + v) + u * v * v) / den;
-    const double f1 = (-w - u * u * u + 2 * u * v) / den;
-    const double f2 = u / den;
-    for (int k = 0; k < 9; k++) inv[k] = f1 * Q[k] + f2 * Q2[k];
-    for (int i = 0; i < 3; i++) inv[i + 3 * i] = inv[i + 3 * i] + Cx<double>(f0, 0);
+    U3Inverse r;
+    u3_inverse_sqrt(Vm, r);
+    mat3_mul(Vm, r.inv, W);
+    mat3_mul(r.Q, r.inv, H);  // H = Q Q^{-1/2}
+    u = r.u;
+    v = r.v;
+    w = r.w;
   }
-  mat3_mul(Vm, inv, W);
-  mat3_mul(Q, inv, H);
-  // skew = W^+ dW - dW^+ W
-  Cx<double> a[9], b[9], rhs[9];
-  mat3_adj_mul(W, dWm, a);
-  mat3_adj_mul(dWm, W, b);
-  for (int k = 0; k < 9; k++) rhs[k] = a[k] - b[k];
-  // system[eq = r + 3c][unknown]: sum_k H[r,k] X[k,c] + sum_k X[r,k] H[k,c]
-  Cx<double> A[9][9];
-  for (int i = 0; i < 9; i++)
-    for (int j = 0; j < 9; j++) A[i][j] = Cx<double>(0, 0);
-  for (int c = 0; c < 3; c++)
-    for (int r = 0; r < 3; r++) {
-      const int eq = r + 3 * c;
-      for (int k = 0; k < 3; k++) {
-        A[eq][k + 3 * c] = A[eq][k + 3 * c] + H[r + 3 * k];
-        A[eq][r + 3 * k] = A[eq][r + 3 * k] + H[k + 3 * c];
-      }
-    }
-  solve9(A, rhs);
-  mat3_mul(W, rhs, a);
+  {
+    Cx<double> dWm[9], a[9];
+    load9(dW + (size_t)mu * 9 * n, n, s, dWm);
+    mat3_adj_mul(W, dWm, C);
+    mat3_adj_mul(dWm, W, a);
+#pragma unroll
+    for (int k = 0; k < 9; k++) C[k] = C[k] - a[k];
+  }
+  Cx<double> X[9];
+  {
+    Cx<double> HC[9], CH[9], t1[9], t2[9];
+    mat3_mul(H, C, HC);
+    mat3_mul(C, H, CH);
+    // v C + u (HC - CH) - H C H, then + H (HC) + (CH) H
+    mat3_mul(HC, H, t1);  // H C H
+#pragma unroll
+    for (int k = 0; k < 9; k++) X[k] = v * C[k] + u * (HC[k] - CH[k]) - t1[k];
+    mat3_mul(H, HC, t1);  // H^2 C
+    mat3_mul(CH, H, t2);  // C H^2
+#pragma unroll
+    for (int k = 0; k < 9; k++) X[k] = X[k] + t1[k] + t2[k];
+    // M = H^3 + u H^2 + v H + w
+    mat3_mul(H, H, t1);   // H^2
+    mat3_mul(t1, H, t2);  // H^3
+#pragma unroll
+    for (int k = 0; k < 9; k++) t2[k] = t2[k] + u * t1[k] + v * H[k];
+    for (int i = 0; i < 3; i++) t2[i + 3 * i] = t2[i + 3 * i] + Cx<double>(w, 0);
+    mat3_inverse(t2, t1);
+    mat3_mul(t1, X, HC);  // X = M^{-1} (...)
+#pragma unroll
+    for (int k = 0; k < 9; k++) X[k] = HC[k];
+  }
+  Cx<double> a[9], b[9];
+  mat3_mul(W, X, a);
   double2 *out = dV + (size_t)mu * 9 * n;
   load9(out, n, s, b);
+#pragma unroll
   for (int k = 0; k < 9; k++) b[k] = b[k] + a[k];
   store9(out, n, s, b);
 }

@@ -179,16 +179,26 @@ __global__ void __launch_bounds__(kSmearThreads)
   store9(Vm, g.V, s, v);
 }
 
-// W = V (V^+V)^{-1/2} (HISQFullSmearing.jl:1-77)
-LMB_D void u3_project(const Cx<double> *Vm, Cx<double> *W) {
+// (V^+V)^{-1/2} for the U(3) projection (HISQFullSmearing.jl:1-77):
+// Q = V^+V, its eigenvalues g0, g1, g2 from the trigonometric solution of
+// the characteristic cubic (coefficients from traces of Q, Q^2, Q^3), each
+// floored at the machine epsilon, and Q^{-1/2} = f0 + f1 Q + f2 Q^2 by
+// Cayley-Hamilton, f_k symmetric functions of sqrt(g_i).  Returns Q, Q^2,
+// Q^{-1/2} and the elementary symmetric functions u, v, w of the sqrt(g_i)
+// (the U(3) pullback needs them).  The smearing and the force share it, so
+// both use the same branch thresholds.
+struct U3Inverse {
   Cx<double> Q[9], Q2[9], inv[9];
-  mat3_adj_mul(Vm, Vm, Q);
-  mat3_mul(Q, Q, Q2);
+  double u, v, w;
+};
+LMB_D void u3_inverse_sqrt(const Cx<double> *Vm, U3Inverse &r) {
+  mat3_adj_mul(Vm, Vm, r.Q);
+  mat3_mul(r.Q, r.Q, r.Q2);
   double c0 = 0, trQ2 = 0, trQ3 = 0;
   for (int i = 0; i < 3; i++) {
-    c0 += Q[i + 3 * i].re;
-    trQ2 += Q2[i + 3 * i].re;
-    for (int j = 0; j < 3; j++) trQ3 += (Q2[i + 3 * j] * Q[j + 3 * i]).re;
+    c0 += r.Q[i + 3 * i].re;
+    trQ2 += r.Q2[i + 3 * i].re;
+    for (int j = 0; j < 3; j++) trQ3 += (r.Q2[i + 3 * j] * r.Q[j + 3 * i]).re;
   }
   const double c1 = trQ2 / 2, c2 = trQ3 / 3;
   double S = c1 / 3 - c0 * c0 / 18;
@@ -219,9 +229,18 @@ LMB_D void u3_project(const Cx<double> *Vm, Cx<double> *W) {
   const double f1 = (-w - u * u * u + 2 * u * v) / den;
   const double f2 = u / den;
 #pragma unroll
-  for (int k = 0; k < 9; k++) inv[k] = f1 * Q[k] + f2 * Q2[k];
-  for (int i = 0; i < 3; i++) inv[i + 3 * i] = inv[i + 3 * i] + Cx<double>(f0, 0);
-  mat3_mul(Vm, inv, W);
+  for (int k = 0; k < 9; k++) r.inv[k] = f1 * r.Q[k] + f2 * r.Q2[k];
+  for (int i = 0; i < 3; i++) r.inv[i + 3 * i] = r.inv[i + 3 * i] + Cx<double>(f0, 0);
+  r.u = u;
+  r.v = v;
+  r.w = w;
+}
+
+// W = V (V^+V)^{-1/2}
+LMB_D void u3_project(const Cx<double> *Vm, Cx<double> *W) {
+  U3Inverse r;
+  u3_inverse_sqrt(Vm, r);
+  mat3_mul(Vm, r.inv, W);
 }
 
 template <int = 0>

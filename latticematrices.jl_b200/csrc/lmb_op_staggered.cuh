@@ -38,6 +38,14 @@ struct StaggeredPolicy {
         if (naik) {
           const Gauge<P> X = gauge_view<P>(ctx->links[LMB_LINKS_FAT], g.V);
           const Gauge<P> Lk = gauge_view<P>(ctx->links[LMB_LINKS_LONG], g.V);
+          if constexpr (PersistentEpi<Epi>::value) {
+            if (ctx->persistent) {
+              auto kern = staggered_adj_persistent_kernel<true, Epi>;
+              const unsigned g2 = std::min(grid2, resident_grid(ctx, kern));
+              kern<<<g2, kStagThreads, 0, st>>>(g, in, X, Lk, mass, fc, lc, epi, (int)grid2);
+              return;
+            }
+          }
           staggered_adj_kernel<true><<<grid2, kStagThreads, 0, st>>>(g, in, X, Lk, mass, fc, lc, epi);
         } else {
           const Gauge<P> X = gauge_view<P>(thin, g.V);

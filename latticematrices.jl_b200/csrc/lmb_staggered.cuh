@@ -274,6 +274,45 @@ LMB_D void stag_hop_adj(const Geom &g, int s0, const int *c0, const int *c1, con
   for (int i = 0; i < 3; i++) acc[i] = Cx2(fma2(-eta, o[i].re, acc[i].re), fma2(-eta, o[i].im, acc[i].im));
 }
 
+// D psi at the x-adjacent sites s0 (x even) and s0 + 1
+template <bool NAIK>
+LMB_D void stag_adj_sites(const Geom &g, int s0, const Field<PREC_SINGLE, 3> &in, const Gauge<PREC_SINGLE> &X,
+                          const Gauge<PREC_SINGLE> &Lk, float mass, float fc, float lc, Cx2 *out) {
+  int c0[4], c1[4];
+  site_coords(g, s0, c0);
+  c1[0] = c0[0] + 1;
+  c1[1] = c0[1];
+  c1[2] = c0[2];
+  c1[3] = c0[3];
+  const int p0 = c0[0] + g.eta_off[0], p1 = p0 + c0[1] + g.eta_off[1], p2 = p1 + c0[2] + g.eta_off[2];
+  const float e1 = (p0 & 1) ? -1.f : 1.f, e2 = (p1 & 1) ? -1.f : 1.f, e3 = (p2 & 1) ? -1.f : 1.f;
+  const float2 eta0 = f2(1.f), eta1 = f2(e1, -e1), eta2 = f2(e2, -e2), eta3 = f2(e3, -e3);
+  Cx2 fat[3] = {cx2_zero(), cx2_zero(), cx2_zero()};
+  stag_hop_adj<0, 1>(g, s0, c0, c1, in, X, eta0, fat);
+  stag_hop_adj<1, 1>(g, s0, c0, c1, in, X, eta1, fat);
+  stag_hop_adj<2, 1>(g, s0, c0, c1, in, X, eta2, fat);
+  stag_hop_adj<3, 1>(g, s0, c0, c1, in, X, eta3, fat);
+  Cx2 psi[3];
+  load_adj(in, s0, psi);
+  const float2 m2 = f2(mass), f2c = f2(fc);
+  if constexpr (NAIK) {
+    Cx2 lng[3] = {cx2_zero(), cx2_zero(), cx2_zero()};
+    stag_hop_adj<0, 3>(g, s0, c0, c1, in, Lk, eta0, lng);
+    stag_hop_adj<1, 3>(g, s0, c0, c1, in, Lk, eta1, lng);
+    stag_hop_adj<2, 3>(g, s0, c0, c1, in, Lk, eta2, lng);
+    stag_hop_adj<3, 3>(g, s0, c0, c1, in, Lk, eta3, lng);
+    const float2 l2 = f2(lc);
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+      out[k] = Cx2(fma2(l2, lng[k].re, fma2(f2c, fat[k].re, m2 * psi[k].re)),
+                   fma2(l2, lng[k].im, fma2(f2c, fat[k].im, m2 * psi[k].im)));
+  } else {
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+      out[k] = Cx2(fma2(f2c, fat[k].re, m2 * psi[k].re), fma2(f2c, fat[k].im, m2 * psi[k].im));
+  }
+}
+
 // V/2 threads.  Epi must provide skip() and pair_adj(s0, active, out[3]).
 template <bool NAIK, class Epi>
 __global__ void __launch_bounds__(kStagThreads, LMB_PAIR_MINB)
@@ -284,42 +323,28 @@ __global__ void __launch_bounds__(kStagThreads, LMB_PAIR_MINB)
   const bool active = i < (int)(g.V >> 1);
   const int s0 = 2 * i;
   Cx2 out[3];
-  if (active) {
-    int c0[4], c1[4];
-    site_coords(g, s0, c0);
-    c1[0] = c0[0] + 1;
-    c1[1] = c0[1];
-    c1[2] = c0[2];
-    c1[3] = c0[3];
-    const int p0 = c0[0] + g.eta_off[0], p1 = p0 + c0[1] + g.eta_off[1], p2 = p1 + c0[2] + g.eta_off[2];
-    const float e1 = (p0 & 1) ? -1.f : 1.f, e2 = (p1 & 1) ? -1.f : 1.f, e3 = (p2 & 1) ? -1.f : 1.f;
-    const float2 eta0 = f2(1.f), eta1 = f2(e1, -e1), eta2 = f2(e2, -e2), eta3 = f2(e3, -e3);
-    Cx2 fat[3] = {cx2_zero(), cx2_zero(), cx2_zero()};
-    stag_hop_adj<0, 1>(g, s0, c0, c1, in, X, eta0, fat);
-    stag_hop_adj<1, 1>(g, s0, c0, c1, in, X, eta1, fat);
-    stag_hop_adj<2, 1>(g, s0, c0, c1, in, X, eta2, fat);
-    stag_hop_adj<3, 1>(g, s0, c0, c1, in, X, eta3, fat);
-    Cx2 psi[3];
-    load_adj(in, s0, psi);
-    const float2 m2 = f2(mass), f2c = f2(fc);
-    if constexpr (NAIK) {
-      Cx2 lng[3] = {cx2_zero(), cx2_zero(), cx2_zero()};
-      stag_hop_adj<0, 3>(g, s0, c0, c1, in, Lk, eta0, lng);
-      stag_hop_adj<1, 3>(g, s0, c0, c1, in, Lk, eta1, lng);
-      stag_hop_adj<2, 3>(g, s0, c0, c1, in, Lk, eta2, lng);
-      stag_hop_adj<3, 3>(g, s0, c0, c1, in, Lk, eta3, lng);
-      const float2 l2 = f2(lc);
-#pragma unroll
-      for (int k = 0; k < 3; k++)
-        out[k] = Cx2(fma2(l2, lng[k].re, fma2(f2c, fat[k].re, m2 * psi[k].re)),
-                     fma2(l2, lng[k].im, fma2(f2c, fat[k].im, m2 * psi[k].im)));
-    } else {
-#pragma unroll
-      for (int k = 0; k < 3; k++)
-        out[k] = Cx2(fma2(f2c, fat[k].re, m2 * psi[k].re), fma2(f2c, fat[k].im, m2 * psi[k].im));
-    }
-  }
+  if (active) stag_adj_sites<NAIK>(g, s0, in, X, Lk, mass, fc, lc, out);
   epi.pair_adj(s0, active, out);
+}
+
+// persistent form for the reducing CG epilogues (as the Wilson pair kernel)
+template <bool NAIK, class Epi>
+__global__ void __launch_bounds__(kStagThreads, LMB_PAIR_MINB)
+    staggered_adj_persistent_kernel(const Geom g, const Field<PREC_SINGLE, 3> in, const Gauge<PREC_SINGLE> X,
+                                    const Gauge<PREC_SINGLE> Lk, const float mass, const float fc, const float lc,
+                                    Epi epi, int ntiles) {
+  if (epi.skip()) return;
+  double red[1] = {0.0};
+  const int npairs = (int)(g.V >> 1);
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int i = tile * kStagThreads + threadIdx.x;
+    const bool active = i < npairs;
+    const int s0 = 2 * i;
+    Cx2 out[3];
+    if (active) stag_adj_sites<NAIK>(g, s0, in, X, Lk, mass, fc, lc, out);
+    epi.pair_adj_acc(s0, active, out, red);
+  }
+  epi.finish(red);
 }
 
 }  // namespace lmb
