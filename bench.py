@@ -99,7 +99,7 @@ def parse():
                          "iteration count (about two minutes on 16 cores at 32^3x64)")
     ap.add_argument("--workload", default="clover",
                     choices=["clover", "wilson8", "hisq", "hisq_dslash", "batched", "force",
-                             "clover_force", "dw", "evenodd"],
+                             "clover_force", "dw", "evenodd", "sharded"],
                     help="clover: 32^3x64 Wilson-clover mixed vs FP64 CG (the "
                          "headline line); wilson8: 8^4 Wilson FP64 CG beside the "
                          "CPU oracle; hisq: 48^3x96 HISQ smearing + CG; batched: "
@@ -109,7 +109,9 @@ def parse():
                          "dw: 16^3x32 x L5 12 Mobius domain-wall D5'D5 CG; evenodd: "
                          "32^3x64 clover D x = b, even/odd Schur solve vs the "
                          "D'D CG route; hisq_dslash: one FP64 HISQ D application "
-                         "at 8^4 .. 32^4 beside the reference's published table")
+                         "at 8^4 .. 32^4 beside the reference's published table; "
+                         "sharded: the clover CG on the native sharded operators "
+                         "(lattice split over the ranks; one rank exchanges with itself)")
     ap.add_argument("--l5", type=int, default=12)
     ap.add_argument("--hisq-sizes", default="8,16,24,32",
                     help="hisq_dslash: lattice extents L of the L^4 lattices")
@@ -118,6 +120,11 @@ def parse():
     ap.add_argument("--samples", type=int, default=9,
                     help="hisq_dslash: timing samples per size")
     ap.add_argument("--fd-directions", type=int, default=64)
+    ap.add_argument("--grid", default="",
+                    help="sharded: process grid a,b,c,d (default 1,1,1,N)")
+    ap.add_argument("--split", default="",
+                    help="sharded: exchanged dimensions as 0/1 flags (default: the grid's "
+                         "dimensions with more than one rank; t on one rank)")
     return ap.parse_args()
 
 
@@ -960,6 +967,123 @@ def run_evenodd(args):
     print(json.dumps(out), flush=True)
 
 
+def run_sharded(args):
+    """The 32^3x64 Wilson-clover D'D CG on the native sharded operators
+    (lmb_set_process_grid): the lattice split over a process grid of the
+    ranks (--grid, default 1,1,1,N), every rank solving its block with faces
+    exchanged over NCCL under the interior sites and every reduction summed
+    over the ranks.  One rank with --split (default t) exchanges its faces
+    with itself: the sharded machinery on one GPU, timed beside the same
+    solve on the unsplit lattice.  Every rank builds the global input (links
+    seed 1, source seed 2, as the headline workload) and keeps its padded
+    block, halo included; strong scaling (the lattice is fixed)."""
+    import ctypes
+
+    import numpy as np
+    import torch
+    import lmb200 as lmb
+    from lmb200._lib import (CGParams, CGResultC, Context, LINKS_THIN, OP_WILSON_CLOVER, PREC)
+    from lmb200.distributed import shared_unique_id
+    from lmb200._lib import nccl_unique_id
+
+    rank, local, ws = dist_setup("nccl")
+    dev = torch.device("cuda", local)
+    L = tuple(int(v) for v in args.lattice.split(","))
+    grid = tuple(int(v) for v in args.grid.split(",")) if args.grid else (1, 1, 1, ws)
+    if int(np.prod(grid)) != ws:
+        raise SystemExit(f"--grid {grid} needs {int(np.prod(grid))} ranks, running {ws}")
+    if args.split:
+        split = tuple(int(v) for v in args.split.split(","))
+    else:
+        split = tuple(int(p > 1) for p in grid) if ws > 1 else (0, 0, 0, 1)
+    PN = tuple(n // p for n, p in zip(L, grid))
+    coords = tuple(int(c) for c in np.unravel_index(rank, grid))
+
+    def nb(d, step):
+        c = list(coords)
+        c[d] = (c[d] + step) % grid[d]
+        return int(np.ravel_multi_index(c, grid))
+
+    Ug = lmb.random_su3_links(L, args.amplitude, 1, nw=1, device=dev)
+    bg = lmb.gaussian_fermion(L, 3, 4, 2, nw=1, phases=PHASES, device=dev)
+    for u in Ug:
+        lmb.set_halo_(u)
+
+    def block(A):
+        # padded block (halo 1) of a padded global field: storage axis 3 - d
+        # is dimension d; global core index g sits at padded index g + 1
+        for d in range(4):
+            if grid[d] == 1:
+                continue
+            lo = coords[d] * PN[d]
+            idx = (torch.arange(lo - 1, lo + PN[d] + 1, device=dev) % L[d]) + 1
+            A = A.index_select(3 - d, idx)
+        return A.contiguous()
+
+    U = [block(u.A) for u in Ug]
+    b = block(bg.A)
+    x = torch.zeros_like(b)
+    del Ug, bg
+    torch.cuda.empty_cache()
+    ctx = Context(local)
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    stream = torch.cuda.current_stream()
+
+    def attach(on):
+        if on:
+            nid = shared_unique_id() if ws > 1 else nccl_unique_id()
+            ctx.set_process_grid(nid, ws, rank, grid, coords, split,
+                                 [nb(d, -1) for d in range(4)], [nb(d, +1) for d in range(4)])
+        else:
+            ctx.set_process_grid(None, 1, 0, (1, 1, 1, 1), (0, 0, 0, 0), (0, 0, 0, 0),
+                                 (0, 0, 0, 0), (0, 0, 0, 0))
+        ctx.set_geometry(PN, 1, PHASES, coords, 0)
+        ctx.upload_links(LINKS_THIN, [u.data_ptr() for u in U], [1, 1, 1, 1], st)
+
+    def solve(prec, profile=False):
+        prm = CGParams()
+        prm.op = OP_WILSON_CLOVER
+        prm.kappa, prm.csw = args.kappa, args.csw
+        prm.rtol, prm.atol, prm.maxiter = args.rtol, 0.0, args.maxiter
+        prm.precision, prm.delta, prm.profile = PREC[prec], args.delta, int(profile)
+        x.zero_()
+        res = CGResultC()
+        ctx.check(ctx.lib.lmb_cg_ddagd(ctx.handle, ctypes.byref(prm), x.data_ptr(), b.data_ptr(),
+                                       ctypes.byref(res), st))
+        return res
+
+    def timed(prec, steps):
+        for _ in range(args.warmup if prec == args.precision else 1):
+            solve(prec)
+        barrier(ws)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        out = [solve(prec, profile=(i == steps - 1)) for i in range(steps)]
+        e.record(stream)
+        torch.cuda.synchronize()
+        barrier(ws)
+        sec = max_over_ranks(s.elapsed_time(e) / 1e3 / steps, ws, dev)
+        r = out[-1]
+        return {"seconds": sec, "iterations": r.iterations, "converged": bool(r.converged),
+                "relative_residual": r.relative_residual,
+                "k1_ms_per_iteration": r.dslash_ms / max(r.dslash_launches, 1),
+                "k2_ms_per_iteration": r.update_ms / max(r.update_launches, 1)}
+
+    attach(True)
+    rows = {"sharded": {p: timed(p, s) for p, s in ((args.precision, args.steps), ("double", args.fp64_steps))}}
+    if ws == 1:   # the same solves on the unsplit lattice
+        attach(False)
+        rows["unsplit"] = {p: timed(p, s) for p, s in ((args.precision, args.steps), ("double", args.fp64_steps))}
+    if rank == 0:
+        print(json.dumps({
+            "workload": f"Wilson-clover D'D CG, {'x'.join(map(str, L))}, kappa {args.kappa}, cSW {args.csw}, "
+                        f"rtol {args.rtol}, native sharded operators",
+            "n_gpus": ws, "grid": grid, "split": split, "block": PN, "scaling": "strong",
+            "rows": rows}), flush=True)
+    ctx.set_process_grid(None, 1, 0, (1, 1, 1, 1), (0, 0, 0, 0), (0, 0, 0, 0), (0, 0, 0, 0), (0, 0, 0, 0))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -971,7 +1095,7 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         {"wilson8": run_wilson8, "hisq": run_hisq, "hisq_dslash": run_hisq_dslash, "batched": run_batched,
          "force": run_force, "clover_force": run_clover_force, "dw": run_dw,
-         "evenodd": run_evenodd}[args.workload](args)
+         "evenodd": run_evenodd, "sharded": run_sharded}[args.workload](args)
 
 
 if __name__ == "__main__":

@@ -328,6 +328,29 @@ int lmb_operator_timing(lmb_ctx *ctx, const lmb_cg_params *params,
                         const void *in, int napply, int dagger,
                         double *ms_per_apply, void *stream);
 
+/* Process grid (the reference's Cartesian decomposition,
+ * LatticeMatrices_core.jl:350-358, with exchange_dim! :742-921 and the
+ * Allreduce of every reduction, LatticeMatrices.jl:1024-1128).  After this
+ * call the context's geometry (lmb_set_geometry: local extents L = the
+ * block, coords = this rank's grid coordinates) is the block of `rank` in a
+ * grid of dims[4] ranks; the dimensions of split_mask (bit mu) exchange
+ * faces with the neighbour ranks nb_minus[mu] / nb_plus[mu] over an NCCL
+ * communicator created from the 128-byte nccl_id (lmb_nccl_unique_id on one
+ * rank, shared by the caller) -- every rank calls it collectively.  A split
+ * dimension may hold one rank (its neighbours are itself).  Then the Wilson,
+ * Wilson-clover, staggered and HISQ applications and lmb_cg_ddagd run on the
+ * block: faces packed by kernels, exchanged on a communication stream while
+ * the interior sites are computed, then the boundary sites from the ghost
+ * layers; each CG reduction is summed over the ranks (one FP64 all-reduce).
+ * The caller's padded links must hold a filled halo (set_halo!) of width >= 1
+ * (Wilson, staggered) or 3 (HISQ).  nccl_id NULL releases the grid.  NCCL is
+ * loaded at run time (libnccl.so.2); LMB_ERR_UNSUPPORTED without it. */
+int lmb_nccl_unique_id(void *id128);
+int lmb_set_process_grid(lmb_ctx *ctx, const void *nccl_id, int nranks,
+                         int rank, const int dims[4], const int coords[4],
+                         unsigned split_mask, const int nb_minus[4],
+                         const int nb_plus[4]);
+
 /* dot(a, b) = sum conj(a) b over the core (LinearAlgebras/linearalgebra_D.jl:
  * 3325-3341) of two padded fields with ncomp complex numbers per site.
  * out[0] = Re, out[1] = Im.  Synchronises the stream. */

@@ -7,6 +7,7 @@
 // lmb_batch_ops.cu and lmb_force_ops.cu.
 #include "lmb_halo.cuh"
 #include "lmb_hisq_smear.cuh"
+#include "lmb_op_dist.cuh"
 #include "lmb_op_dw.cuh"
 #include "lmb_op_staggered.cuh"
 #include "lmb_op_wilson.cuh"
@@ -19,9 +20,9 @@ namespace lmb {
 // ---------------------------------------------------------------------------
 // link caches
 // ---------------------------------------------------------------------------
-int ensure_link_precision(lmb_ctx *ctx, LinkSet &ls, int prec, cudaStream_t st, bool allow_recon) {
-  const int64_t n = 36 * ctx->g.V;
-  const int64_t V = ctx->g.V;
+int ensure_link_precision(lmb_ctx *ctx, LinkSet &ls, int prec, cudaStream_t st, bool allow_recon, int64_t Vset) {
+  const int64_t V = Vset >= 0 ? Vset : ctx->g.V;
+  const int64_t n = 36 * V;
   if (prec != PREC_DOUBLE && !ls.finite())
     return fail(ctx, LMB_ERR_ARG, "gauge links hold a non-finite entry (or one beyond FP32 range): "
                 "FP32 and int16 storage need finite links");
@@ -129,8 +130,14 @@ int ensure_field_strength(lmb_ctx *ctx, cudaStream_t st) {
   if (cc.F_valid && cc.F_links_version == ls.version) return LMB_OK;
   const int64_t V = ctx->g.V;
   if (!cc.F) LMB_CUDA(ctx, cudaMalloc(&cc.F, sizeof(double2) * 54 * V));
-  clover_field_strength_kernel<<<grid_for(6 * V, 128), 128, 0, st>>>(cc.F, ls.d, ctx->g);
-  LMB_CHECK_LAUNCH(ctx);
+  if (ctx->dist && ctx->dist->split) {
+    // a block of a process grid: the leaves reach the neighbours' links
+    const int rc = dist_field_strength(ctx, st);
+    if (rc) return rc;
+  } else {
+    clover_field_strength_kernel<<<grid_for(6 * V, 128), 128, 0, st>>>(cc.F, ls.d, ctx->g);
+    LMB_CHECK_LAUNCH(ctx);
+  }
   cc.F_valid = true;
   cc.F_links_version = ls.version;
   return LMB_OK;
@@ -249,6 +256,18 @@ int check_links_arg(lmb_ctx *ctx, const void *const U[4], const char *what) {
 }
 
 
+// the operator of a whole lattice, or of a block of a process grid
+template <class Fn>
+int with_wilson(const lmb_ctx *ctx, const WilsonPolicy &op, Fn fn) {
+  if (ctx && ctx->dist) return fn(DistWilsonPolicy{op});
+  return fn(op);
+}
+template <class Fn>
+int with_staggered(const lmb_ctx *ctx, const StaggeredPolicy &op, Fn fn) {
+  if (ctx && ctx->dist) return fn(DistStaggeredPolicy{op});
+  return fn(op);
+}
+
 }  // namespace lmb
 
 // ===========================================================================
@@ -290,6 +309,7 @@ void lmb_destroy(lmb_ctx *ctx) {
     cudaFree(bl.f12);
   }
   release_site_caches(ctx);
+  dist_release(ctx);
   cudaFree(ctx->dw_coef);
   cudaFree(ctx->partials);
   cudaFree(ctx->counter);
@@ -349,6 +369,11 @@ int lmb_set_geometry(lmb_ctx *ctx, const int L[4], int nw, const double phase_re
     release_site_caches(ctx);
     ctx->cache_V = V;
   }
+  if (changed && ctx->dist) {  // boundary lists and link ghosts follow the block
+    for (auto &kv : ctx->dist->boundary) cudaFree(kv.second.first);
+    ctx->dist->boundary.clear();
+    for (auto &v : ctx->dist->ghost_of_version) v = ~0ull;
+  }
   return LMB_OK;
 }
 
@@ -404,25 +429,29 @@ int lmb_links_upload(lmb_ctx *ctx, int which, const void *const U[4], const uint
 
 int lmb_wilson_apply(lmb_ctx *ctx, void *out, const void *in, double kappa, int dagger, int precision,
                      void *stream) {
-  return apply_dispatch(ctx, WilsonPolicy{LMB_OP_WILSON, kappa, 0.0}, out, in, dagger, precision, stream);
+  return with_wilson(ctx, WilsonPolicy{LMB_OP_WILSON, kappa, 0.0},
+                     [&](const auto &op) { return apply_dispatch(ctx, op, out, in, dagger, precision, stream); });
 }
 
 int lmb_wilson_clover_apply(lmb_ctx *ctx, void *out, const void *in, double kappa, double csw, int dagger,
                             int precision, void *stream) {
-  return apply_dispatch(ctx, WilsonPolicy{LMB_OP_WILSON_CLOVER, kappa, csw}, out, in, dagger, precision, stream);
+  return with_wilson(ctx, WilsonPolicy{LMB_OP_WILSON_CLOVER, kappa, csw},
+                     [&](const auto &op) { return apply_dispatch(ctx, op, out, in, dagger, precision, stream); });
 }
 
 int lmb_staggered_apply(lmb_ctx *ctx, void *out, const void *in, double mass, int dagger, int precision,
                         void *stream) {
   if (ctx && !std::isfinite(mass)) return fail(ctx, LMB_ERR_ARG, "mass must be finite");
-  return apply_dispatch(ctx, StaggeredPolicy{false, mass, 0.0}, out, in, dagger, precision, stream);
+  return with_staggered(ctx, StaggeredPolicy{false, mass, 0.0},
+                        [&](const auto &op) { return apply_dispatch(ctx, op, out, in, dagger, precision, stream); });
 }
 
 int lmb_hisq_apply(lmb_ctx *ctx, void *out, const void *in, double mass, double naik_epsilon, int dagger,
                    int precision, void *stream) {
   if (ctx && !std::isfinite(mass)) return fail(ctx, LMB_ERR_ARG, "mass must be finite");
   if (ctx && !std::isfinite(naik_epsilon)) return fail(ctx, LMB_ERR_ARG, "naik_epsilon must be finite");
-  return apply_dispatch(ctx, StaggeredPolicy{true, mass, naik_epsilon}, out, in, dagger, precision, stream);
+  return with_staggered(ctx, StaggeredPolicy{true, mass, naik_epsilon},
+                        [&](const auto &op) { return apply_dispatch(ctx, op, out, in, dagger, precision, stream); });
 }
 
 int lmb_clover_field_strength(lmb_ctx *ctx, void *const F[6], void *stream) {
@@ -458,17 +487,19 @@ int lmb_cg_ddagd(lmb_ctx *ctx, const lmb_cg_params *prm, void *x, const void *b,
     return fail(ctx, LMB_ERR_ARG, "reliable-update delta must lie in (0, 1)");
   std::memset(res, 0, sizeof *res);
   cudaStream_t st = as_stream(stream);
+  auto cg = [&](const auto &op) { return cg_dispatch(ctx, prm, op, x, b, res, st); };
   switch (prm->op) {
     case LMB_OP_WILSON:
     case LMB_OP_WILSON_CLOVER:
-      return cg_dispatch(ctx, prm, WilsonPolicy{prm->op, prm->kappa, prm->csw}, x, b, res, st);
+      return with_wilson(ctx, WilsonPolicy{prm->op, prm->kappa, prm->csw}, cg);
     case LMB_OP_STAGGERED:
       if (!std::isfinite(prm->mass)) return fail(ctx, LMB_ERR_ARG, "mass must be finite");
-      return cg_dispatch(ctx, prm, StaggeredPolicy{false, prm->mass, 0.0}, x, b, res, st);
+      return with_staggered(ctx, StaggeredPolicy{false, prm->mass, 0.0}, cg);
     case LMB_OP_HISQ:
       if (!std::isfinite(prm->mass)) return fail(ctx, LMB_ERR_ARG, "mass must be finite");
-      return cg_dispatch(ctx, prm, StaggeredPolicy{true, prm->mass, prm->naik_epsilon}, x, b, res, st);
+      return with_staggered(ctx, StaggeredPolicy{true, prm->mass, prm->naik_epsilon}, cg);
     case LMB_OP_DOMAINWALL:
+      if (ctx->dist) return fail(ctx, LMB_ERR_UNSUPPORTED, "the domain-wall operator takes one rank per lattice");
       return cg_dispatch(ctx, prm, DWPolicy{}, x, b, res, st);
     default: return fail(ctx, LMB_ERR_ARG, "unknown operator %d", prm->op);
   }
@@ -479,17 +510,17 @@ int lmb_operator_timing(lmb_ctx *ctx, const lmb_cg_params *prm, const void *in, 
   if (!ctx_ok(ctx)) return LMB_ERR_ARG;
   if (!prm || !in || !ms_per_apply) return fail(ctx, LMB_ERR_ARG, "null argument");
   const int prec = prm->precision;
+  auto timing = [&](const auto &op) {
+    return time_dispatch(ctx, op, in, napply, dagger, prec, ms_per_apply, stream);
+  };
   switch (prm->op) {
     case LMB_OP_WILSON:
     case LMB_OP_WILSON_CLOVER:
-      return time_dispatch(ctx, WilsonPolicy{prm->op, prm->kappa, prm->csw}, in, napply, dagger, prec, ms_per_apply,
-                           stream);
+      return with_wilson(ctx, WilsonPolicy{prm->op, prm->kappa, prm->csw}, timing);
     case LMB_OP_STAGGERED:
-      return time_dispatch(ctx, StaggeredPolicy{false, prm->mass, 0.0}, in, napply, dagger, prec, ms_per_apply,
-                           stream);
+      return with_staggered(ctx, StaggeredPolicy{false, prm->mass, 0.0}, timing);
     case LMB_OP_HISQ:
-      return time_dispatch(ctx, StaggeredPolicy{true, prm->mass, prm->naik_epsilon}, in, napply, dagger, prec,
-                           ms_per_apply, stream);
+      return with_staggered(ctx, StaggeredPolicy{true, prm->mass, prm->naik_epsilon}, timing);
     case LMB_OP_DOMAINWALL:
       return time_dispatch(ctx, DWPolicy{}, in, napply, dagger, prec, ms_per_apply, stream);
     default: return fail(ctx, LMB_ERR_ARG, "unknown operator %d", prm->op);
@@ -619,6 +650,7 @@ int lmb_domainwall_set(lmb_ctx *ctx, int L5, double mass, double M, const double
 }
 
 int lmb_domainwall_apply(lmb_ctx *ctx, void *out, const void *in, int dagger, int precision, void *stream) {
+  if (ctx && ctx->dist) return fail(ctx, LMB_ERR_UNSUPPORTED, "the domain-wall operator takes one rank per lattice");
   return apply_dispatch(ctx, DWPolicy{}, out, in, dagger, precision, stream);
 }
 

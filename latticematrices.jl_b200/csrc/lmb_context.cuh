@@ -76,8 +76,11 @@ struct lmb_batch_tune {
   double ms = 0;
 };
 
+struct lmb_dist;  // process grid, NCCL communicator, ghost buffers (lmb_dist_host.cuh)
+
 struct lmb_ctx {
   int device = 0;
+  lmb_dist *dist = nullptr;  // set by lmb_set_process_grid
   std::deque<lmb_batch_links> batch_links;  // deque: element addresses stay valid on growth
   std::map<std::string, lmb_batch_tune> batch_tune;
   lmb_smear_key smear;  // thin links the HISQ fat/long link sets were built from

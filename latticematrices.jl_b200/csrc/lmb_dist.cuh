@@ -1,0 +1,358 @@
+// lmb_dist.cuh -- device side of the sharded (process-grid) operators.
+//
+// A rank holds the block of its Cartesian coordinates (the reference's
+// LatticeMatrix PN block, LatticeMatrices_core.jl:350-358).  Along every
+// exchanged ("split") dimension mu a stencil application
+//   1. packs the rank's two faces of `depth` layers (1 for Wilson, 3 for the
+//      HISQ Naik term) into send buffers -- the minus face multiplied by the
+//      boundary phase when the rank holds global coordinate 0, the plus face by
+//      1/phase when it holds the last one, the rule of exchange_dim!
+//      (LatticeMatrices_core.jl:742-921) --
+//   2. sends them to the two neighbours and receives their faces into ghost
+//      buffers (NCCL, on a communication stream), while
+//   3. an interior kernel computes every site whose neighbours are all local,
+//   4. then a boundary kernel computes the remaining sites, reading the ghost
+//      layers for hops that leave the block (no phase: the sender applied it).
+// Dimensions that are not split wrap in-kernel with the phase, as on one GPU.
+//
+// Ghost layout: a ghost (or face) buffer of dimension mu is a Field of
+// depth * F_mu sites in the storage format of the stencil's field (planes,
+// int16 norms), F_mu = V / L_mu; element (layer j, face index f) sits at
+// j * F_mu + f, f lexicographic (x fastest) over the three other dimensions.
+// Minus ghost layer j holds x_mu = -1 - j, plus ghost layer j holds
+// x_mu = L_mu + j.  Link ghosts hold U_mu (direction mu only) at
+// x_mu = -1 - j, read from the halo the caller filled in the padded links.
+#pragma once
+#include "lmb_pack.cuh"
+#include "lmb_solver.cuh"
+#include "lmb_staggered.cuh"
+#include "lmb_wilson.cuh"
+
+namespace lmb {
+
+struct DistView {
+  unsigned split;   // bit mu: dimension mu exchanged with neighbours
+  int depth;        // ghost layers
+  int face[4];      // F_mu
+  int fstr[4][4];   // stride of dimension nu in the face index of dimension mu (0 for nu == mu)
+};
+
+LMB_D int face_index(const DistView &dv, const int *c, int mu) {
+  return dv.fstr[mu][0] * c[0] + dv.fstr[mu][1] * c[1] + dv.fstr[mu][2] * c[2] + dv.fstr[mu][3] * c[3];
+}
+
+template <int P, int NC>
+struct GhostSpinors {
+  Field<P, NC> m[4], p[4];
+};
+template <class G>
+struct GhostLinks {
+  G m[4];
+};
+
+// a site is interior when every hop of reach `depth` stays in the block
+LMB_D bool dist_interior(const Geom &g, const DistView &dv, const int *c) {
+#pragma unroll
+  for (int mu = 0; mu < 4; mu++)
+    if (((dv.split >> mu) & 1) && (c[mu] < dv.depth || c[mu] >= g.L[mu] - dv.depth)) return false;
+  return true;
+}
+
+// spinor at distance d (|d| <= depth) along MU from site s: a split
+// dimension reads a ghost layer past the block (*wrap = 0), any other
+// dimension wraps periodically (*wrap = signed number of edge crossings)
+template <int P, int NC, typename R>
+LMB_D void load_nb(const Field<P, NC> &in, const GhostSpinors<P, NC> &gh, const Geom &g, const DistView &dv,
+                   int s, const int *c, int MU, int d, Cx<R> *v, int *wrap) {
+  const int L = g.L[MU];
+  int x = c[MU] + d;
+  if ((dv.split >> MU) & 1) {
+    *wrap = 0;
+    if (x >= 0 && x < L) {
+      in.load(s + d * g.stride[MU], v);
+    } else {
+      const int f = face_index(dv, c, MU);
+      if (x >= L) gh.p[MU].load((int64_t)(x - L) * dv.face[MU] + f, v);
+      else gh.m[MU].load((int64_t)(-1 - x) * dv.face[MU] + f, v);
+    }
+    return;
+  }
+  int w = 0;
+  while (x >= L) {
+    x -= L;
+    w++;
+  }
+  while (x < 0) {
+    x += L;
+    w--;
+  }
+  *wrap = w;
+  in.load(s + (x - c[MU]) * g.stride[MU], v);
+}
+
+// link U_MU at site x + d MU, d <= 0 (backward hops)
+template <class G, typename R>
+LMB_D void load_link_nb(const G &U, const GhostLinks<G> &gu, const Geom &g, const DistView &dv, int s,
+                        const int *c, int MU, int d, Cx<R> *u) {
+  const int L = g.L[MU];
+  int x = c[MU] + d;
+  if (((dv.split >> MU) & 1) && x < 0) {
+    gu.m[MU].load(MU, (int64_t)(-1 - x) * dv.face[MU] + face_index(dv, c, MU), u);
+    return;
+  }
+  while (x < 0) x += L;
+  U.load(MU, s + (x - c[MU]) * g.stride[MU], u);
+}
+
+// ---------------------------------------------------------------------------
+// face packing: minus face (x_mu = j) -> send_m, plus face (x_mu = L-1-j) ->
+// send_p, each multiplied by its phase factor (1 unless the rank holds the
+// global edge)
+// ---------------------------------------------------------------------------
+template <int P, int NC>
+__global__ void __launch_bounds__(256)
+    pack_faces_kernel(const Field<P, NC> in, Field<P, NC> send_m, Field<P, NC> send_p, const Geom g,
+                      const DistView dv, int mu, double2 ph_m, double2 ph_p) {
+  typedef typename Real<P>::type R;
+  const int64_t F = dv.face[mu];
+  const int64_t t = (int64_t)blockIdx.x * 256 + threadIdx.x;
+  if (t >= dv.depth * F) return;
+  const int layer = (int)(t / F);
+  int f = (int)(t - layer * F);
+  int c[4];
+#pragma unroll
+  for (int nu = 0; nu < 4; nu++) {
+    if (nu == mu) continue;
+    c[nu] = f % g.L[nu];
+    f /= g.L[nu];
+  }
+  Cx<R> v[NC];
+  c[mu] = layer;
+  int s = c[0] + g.stride[1] * c[1] + g.stride[2] * c[2] + g.stride[3] * c[3];
+  in.load(s, v);
+  if (ph_m.x != 1.0 || ph_m.y != 0.0) {
+    const Cx<R> ph((R)ph_m.x, (R)ph_m.y);
+#pragma unroll
+    for (int k = 0; k < NC; k++) v[k] = v[k] * ph;
+  }
+  send_m.store(t, v);
+  c[mu] = g.L[mu] - 1 - layer;
+  s = c[0] + g.stride[1] * c[1] + g.stride[2] * c[2] + g.stride[3] * c[3];
+  in.load(s, v);
+  if (ph_p.x != 1.0 || ph_p.y != 0.0) {
+    const Cx<R> ph((R)ph_p.x, (R)ph_p.y);
+#pragma unroll
+    for (int k = 0; k < NC; k++) v[k] = v[k] * ph;
+  }
+  send_p.store(t, v);
+}
+
+// link ghost of dimension mu from the caller's padded links (halo filled):
+// U_mu at x_mu = -1 - j into direction mu's 9 planes of a 36-plane buffer
+template <typename T>
+__global__ void __launch_bounds__(256)
+    pack_link_ghost_kernel(double2 *dst, const T *Umu, const Geom g, const Padded pd, const DistView dv, int mu) {
+  const int64_t F = dv.face[mu], Vg = dv.depth * F;
+  const int64_t t = (int64_t)blockIdx.x * 256 + threadIdx.x;
+  if (t >= Vg) return;
+  const int layer = (int)(t / F);
+  int f = (int)(t - layer * F);
+  int c[4];
+#pragma unroll
+  for (int nu = 0; nu < 4; nu++) {
+    if (nu == mu) continue;
+    c[nu] = f % g.L[nu];
+    f /= g.L[nu];
+  }
+  c[mu] = -1 - layer;
+  const int64_t ps = padded_site(pd, c) * 9;
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    const T v = Umu[ps + k];
+    dst[(mu * 9 + k) * Vg + t] = make_double2((double)v.x, (double)v.y);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Wilson / Wilson-clover, one site per thread
+// ---------------------------------------------------------------------------
+template <typename R, int DAG, int MU, int P, class G>
+LMB_D void hop_dir_dist(const Geom &g, const DistView &dv, int s, const int *c, const Field<P, 12> &in,
+                        const GhostSpinors<P, 12> &gh, const G &U, const GhostLinks<G> &gu, Cx<R> *acc) {
+  constexpr int FPM = DAG ? +1 : -1;
+  constexpr int BPM = -FPM;
+  Cx<R> p[12], h[6], uh[6], u[9];
+  int w;
+  load_nb(in, gh, g, dv, s, c, MU, 1, p, &w);
+  project<FPM, MU>(p, h);
+  if (w && ((g.phase_mask >> MU) & 1)) scale_phase(h, 6, g.ph_fwd[MU]);
+  U.load(MU, s, u);
+  su3_mul_half(u, h, uh);
+  reconstruct<FPM, MU>(acc, uh);
+  load_nb(in, gh, g, dv, s, c, MU, -1, p, &w);
+  project<BPM, MU>(p, h);
+  if (w && ((g.phase_mask >> MU) & 1)) scale_phase(h, 6, g.ph_bwd[MU]);
+  load_link_nb(U, gu, g, dv, s, c, MU, -1, u);
+  su3_adj_mul_half(u, h, uh);
+  reconstruct<BPM, MU>(acc, uh);
+}
+
+// interior sites (every neighbour local) with the single-lattice hops
+template <typename R, int DAG, bool CLOVER, int PHM, int P, class G, class CL, class Epi>
+__global__ void __launch_bounds__(kDslashThreads)
+    wilson_interior_kernel(const Geom g, const DistView dv, const Field<P, 12> in, const G U, const CL A,
+                           const R kappa, Epi epi) {
+  if (epi.skip()) return;
+  const int s = blockIdx.x * kDslashThreads + threadIdx.x;
+  bool active = s < g.V;
+  Cx<R> out[12];
+  int c[4];
+  if (active) {
+    site_coords(g, s, c);
+    active = dist_interior(g, dv, c);
+  }
+  if (active) wilson_site_out<R, DAG, CLOVER, PHM>(g, s, c, in, U, A, kappa, out);
+  epi(s, active, out);
+}
+
+// the sites of `list` (the block's boundary), ghost-aware
+template <typename R, int DAG, bool CLOVER, int P, class G, class CL, class Epi>
+__global__ void __launch_bounds__(kDslashThreads)
+    wilson_boundary_kernel(const Geom g, const DistView dv, const Field<P, 12> in, const GhostSpinors<P, 12> gh,
+                           const G U, const GhostLinks<G> gu, const CL A, const R kappa, Epi epi, const int *list,
+                           int n) {
+  if (epi.skip()) return;
+  const int i = blockIdx.x * kDslashThreads + threadIdx.x;
+  const bool active = i < n;
+  const int s = active ? list[i] : 0;
+  Cx<R> out[12];
+  if (active) {
+    int c[4];
+    site_coords(g, s, c);
+    Cx<R> acc[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) acc[k] = Cx<R>(0, 0);
+    hop_dir_dist<R, DAG, 0>(g, dv, s, c, in, gh, U, gu, acc);
+    hop_dir_dist<R, DAG, 1>(g, dv, s, c, in, gh, U, gu, acc);
+    hop_dir_dist<R, DAG, 2>(g, dv, s, c, in, gh, U, gu, acc);
+    hop_dir_dist<R, DAG, 3>(g, dv, s, c, in, gh, U, gu, acc);
+    wilson_site_finish<R, CLOVER>(s, in, A, kappa, acc, out);
+  }
+  epi(s, active, out);
+}
+
+// ---------------------------------------------------------------------------
+// staggered / HISQ, one site per thread
+// ---------------------------------------------------------------------------
+template <typename R, int MU, int D, int P, class G>
+LMB_D void stag_hop_dist(const Geom &g, const DistView &dv, int s, const int *c, const Field<P, 3> &in,
+                         const GhostSpinors<P, 3> &gh, const G &U, const GhostLinks<G> &gu, R eta, Cx<R> *acc) {
+  Cx<R> v[3], u[9], o[3];
+  int w;
+  load_nb(in, gh, g, dv, s, c, MU, D, v, &w);
+  apply_wraps(g, MU, w, v);
+  U.load(MU, s, u);
+  su3_mul_vec(u, v, o);
+#pragma unroll
+  for (int i = 0; i < 3; i++) acc[i] = acc[i] + eta * o[i];
+  load_nb(in, gh, g, dv, s, c, MU, -D, v, &w);
+  apply_wraps(g, MU, w, v);
+  load_link_nb(U, gu, g, dv, s, c, MU, -D, u);
+  su3_adj_mul_vec(u, v, o);
+#pragma unroll
+  for (int i = 0; i < 3; i++) acc[i] = acc[i] - eta * o[i];
+}
+
+template <typename R, bool NAIK, int PHM, int P, class GF, class GL, class Epi>
+__global__ void __launch_bounds__(kStagThreads)
+    staggered_interior_kernel(const Geom g, const DistView dv, const Field<P, 3> in, const GF X, const GL Lk,
+                              const R mass, const R fc, const R lc, Epi epi) {
+  if (epi.skip()) return;
+  const int s = blockIdx.x * kStagThreads + threadIdx.x;
+  bool active = s < g.V;
+  Cx<R> out[3];
+  if (active) {
+    int c[4];
+    site_coords(g, s, c);
+    active = dist_interior(g, dv, c);
+  }
+  if (active) stag_site<R, NAIK, PHM>(g, s, in, X, Lk, mass, fc, lc, out);
+  epi(s, active, out);
+}
+
+template <typename R, bool NAIK, int P, class GF, class GL, class Epi>
+__global__ void __launch_bounds__(kStagThreads)
+    staggered_boundary_kernel(const Geom g, const DistView dv, const Field<P, 3> in, const GhostSpinors<P, 3> gh,
+                              const GF X, const GhostLinks<GF> gx, const GL Lk, const GhostLinks<GL> gl,
+                              const R mass, const R fc, const R lc, Epi epi, const int *list, int n) {
+  if (epi.skip()) return;
+  const int i = blockIdx.x * kStagThreads + threadIdx.x;
+  const bool active = i < n;
+  const int s = active ? list[i] : 0;
+  Cx<R> out[3];
+  if (active) {
+    int c[4];
+    site_coords(g, s, c);
+    const int p0 = c[0] + g.eta_off[0], p1 = p0 + c[1] + g.eta_off[1], p2 = p1 + c[2] + g.eta_off[2];
+    const R eta[4] = {(R)1, (p0 & 1) ? (R)-1 : (R)1, (p1 & 1) ? (R)-1 : (R)1, (p2 & 1) ? (R)-1 : (R)1};
+    Cx<R> fat[3] = {Cx<R>(0, 0), Cx<R>(0, 0), Cx<R>(0, 0)};
+    stag_hop_dist<R, 0, 1>(g, dv, s, c, in, gh, X, gx, eta[0], fat);
+    stag_hop_dist<R, 1, 1>(g, dv, s, c, in, gh, X, gx, eta[1], fat);
+    stag_hop_dist<R, 2, 1>(g, dv, s, c, in, gh, X, gx, eta[2], fat);
+    stag_hop_dist<R, 3, 1>(g, dv, s, c, in, gh, X, gx, eta[3], fat);
+    Cx<R> psi[3];
+    in.load(s, psi);
+    if constexpr (NAIK) {
+      Cx<R> lng[3] = {Cx<R>(0, 0), Cx<R>(0, 0), Cx<R>(0, 0)};
+      stag_hop_dist<R, 0, 3>(g, dv, s, c, in, gh, Lk, gl, eta[0], lng);
+      stag_hop_dist<R, 1, 3>(g, dv, s, c, in, gh, Lk, gl, eta[1], lng);
+      stag_hop_dist<R, 2, 3>(g, dv, s, c, in, gh, Lk, gl, eta[2], lng);
+      stag_hop_dist<R, 3, 3>(g, dv, s, c, in, gh, Lk, gl, eta[3], lng);
+#pragma unroll
+      for (int k = 0; k < 3; k++) out[k] = mass * psi[k] + fc * fat[k] + lc * lng[k];
+    } else {
+#pragma unroll
+      for (int k = 0; k < 3; k++) out[k] = mass * psi[k] + fc * fat[k];
+    }
+  }
+  epi(s, active, out);
+}
+
+// the scalar step after the sum over the ranks: sums[0] + sums[1] are the
+// interior and boundary kernels' totals
+template <class Epi>
+__global__ void dist_finalize_kernel(Epi epi, const double *sums) {
+  if (epi.skip()) return;  // a paused solve skipped the stencils as well
+  if (threadIdx.x == 0 && blockIdx.x == 0) epi.finalize(sums[0] + sums[1]);
+}
+
+// the whole padded block of the caller's links (halo filled) as 36 planes of
+// a lattice of the padded extents (site order of the padded array)
+template <typename T>
+__global__ void __launch_bounds__(256)
+    padded_block_links_kernel(double2 *dst, const T *U0, const T *U1, const T *U2, const T *U3, int64_t Vp) {
+  const int64_t t = (int64_t)blockIdx.x * 256 + threadIdx.x;
+  if (t >= Vp) return;
+  const T *U[4] = {U0, U1, U2, U3};
+#pragma unroll
+  for (int mu = 0; mu < 4; mu++)
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      const T v = U[mu][t * 9 + k];
+      dst[(mu * 9 + k) * Vp + t] = make_double2((double)v.x, (double)v.y);
+    }
+}
+
+// core sites of 54 field-strength planes computed on the padded block
+template <int = 0>
+__global__ void __launch_bounds__(256)
+    core_of_padded_kernel(double2 *F, const double2 *Fp, const Geom g, const Padded pd, int64_t Vp) {
+  const int s = blockIdx.x * 256 + threadIdx.x;
+  if (s >= g.V) return;
+  int c[4];
+  site_coords(g, s, c);
+  const int64_t ps = padded_site(pd, c);
+  for (int k = 0; k < 54; k++) F[k * g.V + s] = Fp[k * Vp + ps];
+}
+
+}  // namespace lmb

@@ -17,6 +17,10 @@ template <class Op, int PS, int NC>
 int op_pack_in(lmb_ctx *ctx, const Op &, Field<PS, NC> &f, const void *src, cudaStream_t st) {
   return pack_in(ctx, f, src, st);
 }
+// operators on a block of a process grid: device slots for partial sums
+// (nullptr: a whole lattice) and their sum over the ranks
+template <class Op> double *op_local_sums(const lmb_ctx *, const Op &) { return nullptr; }
+template <class Op> int op_allreduce_sums(lmb_ctx *, const Op &, cudaStream_t) { return LMB_OK; }
 template <class Op, int PS, int NC>
 int op_unpack_out(lmb_ctx *ctx, const Op &, void *dst, const Field<PS, NC> &f, cudaStream_t st) {
   return unpack_out(ctx, dst, f, st);
@@ -191,13 +195,20 @@ int cg_run(lmb_ctx *ctx, const lmb_cg_params *prm, const Op &op, void *x_pad, co
     if (xl.norm) LMB_CUDA(ctx, cudaMemsetAsync(xl.norm, 0, Field<PX, NC>::norm_bytes(V), st));
   }
   norm_bx_kernel<NC><<<bgrid, kBlasThreads, 0, st>>>(b64, x64, ctx->st_dev, V, prm->rtol, prm->atol,
-                                                      ctx->partials, ctx->counter);
+                                                      ctx->partials, ctx->counter, op_local_sums(ctx, op));
   LMB_CHECK_LAUNCH(ctx);
   nl++;
+  if (op_local_sums(ctx, op)) {  // a block of a process grid: sum |b|^2, |x0|^2 over the ranks
+    rc = op_allreduce_sums(ctx, op, st);
+    if (rc) return rc;
+    set_norms_kernel<<<1, 32, 0, st>>>(ctx->st_dev, op_local_sums(ctx, op), prm->rtol, prm->atol);
+    LMB_CHECK_LAUNCH(ctx);
+  }
   rc = read_state(ctx, st);
   if (rc) return rc;
-  // b - D'D 0 = b needs finite links (NaN * 0 is NaN)
-  const bool zero_guess = ctx->st_host->xx == 0.0 && finite_links;
+  // b - D'D 0 = b needs finite links (NaN * 0 is NaN); on a process grid the
+  // shortcut's local |b|^2 would need a sum over the ranks, so it is skipped
+  const bool zero_guess = ctx->st_host->xx == 0.0 && finite_links && !op_local_sums(ctx, op);
   // r = b - D'D x (FP64)
   auto true_residual = [&](int mode) -> int {
     EpiStore<PREC_DOUBLE, NC> e1{t64, nullptr};

@@ -36,7 +36,9 @@ inline int check_prec(lmb_ctx *ctx, int prec) {
 }
 
 // link and clover caches (lmb_capi.cu)
-int ensure_link_precision(lmb_ctx *ctx, LinkSet &ls, int prec, cudaStream_t st, bool allow_recon = true);
+// Vset: volume of the set (default: the context's)
+int ensure_link_precision(lmb_ctx *ctx, LinkSet &ls, int prec, cudaStream_t st, bool allow_recon = true,
+                          int64_t Vset = -1);
 float device_absmax(lmb_ctx *ctx, const double2 *p, int64_t n, cudaStream_t st, int *rc);
 int ensure_field_strength(lmb_ctx *ctx, cudaStream_t st);
 int ensure_clover(lmb_ctx *ctx, double coef, int prec, cudaStream_t st);
@@ -46,6 +48,8 @@ int pack_links_to(lmb_ctx *ctx, double2 *dst, const void *const U[4], cudaStream
 int unpack_links_from(lmb_ctx *ctx, void *const U[4], const double2 *src, cudaStream_t st);
 int check_links_arg(lmb_ctx *ctx, const void *const U[4], const char *what);
 void release_site_caches(lmb_ctx *ctx);
+// F_mu_nu of a process-grid block from the caller's halo-filled links (lmb_dist_ops.cu)
+int dist_field_strength(lmb_ctx *ctx, cudaStream_t st);
 // even/odd caches (lmb_schur_ops.cu)
 int ensure_clover_inverse(lmb_ctx *ctx, int prec, cudaStream_t st);
 int ensure_eo_copies(lmb_ctx *ctx, int prec, bool clover, cudaStream_t st);

@@ -140,15 +140,21 @@ struct EpiStoreNorm {  // K1
   CGState *st;
   double *partials;
   unsigned *counter;
+  // set by the sharded operators: the grid's sum goes to *local (summed
+  // over the ranks and passed to finalize() afterwards) instead of finalize
+  double *local = nullptr;
   LMB_D bool skip() const { return ((volatile CGState *)st)->status != ST_RUNNING; }
+  LMB_D void finalize(double total) const { finalize_pAp(st, total); }
   template <typename R> LMB_D void operator()(int s, bool active, const Cx<R> *v) const {
     double n2[1] = {0.0}, tot[1];
     if (active) {
       out.store(s, v);
       n2[0] = sum_norm2(v, NC);
     }
-    if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0)
-      finalize_pAp(st, tot[0]);
+    if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0) {
+      if (local) *local = tot[0];
+      else finalize_pAp(st, tot[0]);
+    }
   }
   LMB_D void pair_adj(int s0, bool active, const Cx2 *v) const {
     double n2[1] = {0.0};
@@ -196,7 +202,9 @@ struct EpiCGUpdate {  // K2
   CGState *st;
   double *partials;
   unsigned *counter;
+  double *local = nullptr;  // as EpiStoreNorm::local
   LMB_D bool skip() const { return ((volatile CGState *)st)->status != ST_RUNNING; }
+  LMB_D void finalize(double total) const { finalize_rr(st, total); }
   template <typename R> LMB_D void operator()(int s, bool active, const Cx<R> *v) const {
     double n2[1] = {0.0}, tot[1];
     if (active) {
@@ -214,8 +222,10 @@ struct EpiCGUpdate {  // K2
       x.store(s, xv);
       n2[0] = sum_norm2(rv, NC);
     }
-    if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0)
-      finalize_rr(st, tot[0]);
+    if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0) {
+      if (local) *local = tot[0];
+      else finalize_rr(st, tot[0]);
+    }
   }
   LMB_D void pair_adj(int s0, bool active, const Cx2 *v) const {
     double n2[1] = {0.0};
@@ -298,7 +308,9 @@ struct EpiResidualNorm {
   double *partials;
   unsigned *counter;
   double *out;
+  double *local = nullptr;  // as EpiStoreNorm::local
   LMB_D bool skip() const { return false; }
+  LMB_D void finalize(double total) const { *out = total; }
   template <typename R> LMB_D void operator()(int s, bool active, const Cx<R> *v) const {
     double n2[1] = {0.0}, tot[1];
     if (active) {
@@ -310,7 +322,10 @@ struct EpiResidualNorm {
         n2[0] += dr * dr + di * di;
       }
     }
-    if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0) *out = tot[0];
+    if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0) {
+      if (local) *local = tot[0];
+      else *out = tot[0];
+    }
   }
 };
 
@@ -324,7 +339,9 @@ struct EpiTrueResidual {
   CGState *st;
   double *partials;
   unsigned *counter;
+  double *local = nullptr;  // as EpiStoreNorm::local
   LMB_D bool skip() const { return false; }
+  LMB_D void finalize(double total) const { finalize_true(st, total, mode); }
   template <typename R> LMB_D void operator()(int s, bool active, const Cx<R> *v) const {
     double n2[1] = {0.0}, tot[1];
     if (active) {
@@ -336,10 +353,20 @@ struct EpiTrueResidual {
       if (write_low) r_low.store(s, rv);
       n2[0] = sum_norm2(rv, NC);
     }
-    if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0)
-      finalize_true(st, tot[0], mode);
+    if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0) {
+      if (local) *local = tot[0];
+      else finalize_true(st, tot[0], mode);
+    }
   }
 };
+
+// epilogues whose kernels end in a grid reduction (a `local` slot and
+// finalize(total)); the sharded operators sum the slot over the ranks
+template <class Epi> struct ReducingEpi { static constexpr bool value = false; };
+template <int PS, int NC> struct ReducingEpi<EpiStoreNorm<PS, NC>> { static constexpr bool value = true; };
+template <int PS, int PX, int NC> struct ReducingEpi<EpiCGUpdate<PS, PX, NC>> { static constexpr bool value = true; };
+template <int NC> struct ReducingEpi<EpiResidualNorm<NC>> { static constexpr bool value = true; };
+template <int PS, int NC> struct ReducingEpi<EpiTrueResidual<PS, NC>> { static constexpr bool value = true; };
 
 // ---------------------------------------------------------------------------
 // vector kernels
@@ -420,7 +447,7 @@ __global__ void __launch_bounds__(kBlasThreads)
 template <int NC>
 __global__ void __launch_bounds__(kBlasThreads)
     norm_bx_kernel(const Field<PREC_DOUBLE, NC> b, const Field<PREC_DOUBLE, NC> x, CGState *st, int64_t V,
-                   double rtol, double atol, double *partials, unsigned *counter) {
+                   double rtol, double atol, double *partials, unsigned *counter, double *local2 = nullptr) {
   const int64_t s = (int64_t)blockIdx.x * kBlasThreads + threadIdx.x;
   double n2[2] = {0.0, 0.0}, tot[2];
   if (s < V) {
@@ -433,12 +460,27 @@ __global__ void __launch_bounds__(kBlasThreads)
     for (int k = 0; k < NC; k++) n2[1] += norm2(v[k]);
   }
   if (grid_reduce<kBlasThreads, 2>(n2, partials, counter, tot) && threadIdx.x == 0) {
+    if (local2) {  // a block of a process grid: summed over the ranks first
+      local2[0] = tot[0];
+      local2[1] = tot[1];
+      return;
+    }
     st->bb = tot[0];
     st->xx = tot[1];
     const double bn = sqrt(tot[0]);
     const double tol = fmax(atol, rtol * bn);
     st->tol2 = tol * tol;
   }
+}
+
+// |b|^2, |x0|^2 and the tolerance from the sums over the ranks
+template <int = 0>
+__global__ void set_norms_kernel(CGState *st, const double *sums, double rtol, double atol) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  st->bb = sums[0];
+  st->xx = sums[1];
+  const double tol = fmax(atol, rtol * sqrt(sums[0]));
+  st->tol2 = tol * tol;
 }
 
 // the initial residual of a zero guess: r = b, r_low = r (optional),

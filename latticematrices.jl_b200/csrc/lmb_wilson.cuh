@@ -212,6 +212,43 @@ LMB_D void wilson_site(const Geom &g, int s, const SF &in, const G &U, R kappa, 
   for (int k = 0; k < 12; k++) out[k] = p[k] - kappa * acc[k];
 }
 
+// out = A psi(s) - kappa acc (A = 1 without the clover term)
+template <typename R, bool CLOVER, class SF, class CL>
+LMB_D void wilson_site_finish(int s, const SF &in, const CL &A, R kappa, const Cx<R> *acc, Cx<R> *out) {
+  Cx<R> p[12];
+  in.load(s, p);
+  if constexpr (CLOVER) {
+    R a[36];
+    Cx<R> v[6], o[6];
+#pragma unroll
+    for (int blk = 0; blk < 2; blk++) {
+      A.load(blk, s, a);
+#pragma unroll
+      for (int k = 0; k < 6; k++) v[k] = p[6 * blk + k];
+      herm6_mul(a, v, o);
+#pragma unroll
+      for (int k = 0; k < 6; k++) out[6 * blk + k] = o[k] - kappa * acc[6 * blk + k];
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 12; k++) out[k] = p[k] - kappa * acc[k];
+  }
+}
+
+// D psi (or D^+ psi) at site s with coordinates c (one site per thread)
+template <typename R, int DAG, bool CLOVER, int PHM, class SF, class G, class CL>
+LMB_D void wilson_site_out(const Geom &g, int s, const int *c, const SF &in, const G &U, const CL &A, R kappa,
+                           Cx<R> *out) {
+  Cx<R> acc[12];
+#pragma unroll
+  for (int k = 0; k < 12; k++) acc[k] = Cx<R>(0, 0);
+  hop_dir<R, DAG, 0, PHM>(g, s, c, in, U, acc);
+  hop_dir<R, DAG, 1, PHM>(g, s, c, in, U, acc);
+  hop_dir<R, DAG, 2, PHM>(g, s, c, in, U, acc);
+  hop_dir<R, DAG, 3, PHM>(g, s, c, in, U, acc);
+  wilson_site_finish<R, CLOVER>(s, in, A, kappa, acc, out);
+}
+
 // The Wilson(-clover) kernel.  Epi must provide:
 //   bool skip() const                      -- whole grid exits (paused solve)
 //   void operator()(s, active, out[12])    -- consume the result
@@ -226,34 +263,11 @@ __global__ void __launch_bounds__(kDslashThreads, LMB_DSLASH_MINB)
   if (active) {
     int c[4];
     site_coords(g, s, c);
-    Cx<R> acc[12];
-#pragma unroll
-    for (int k = 0; k < 12; k++) acc[k] = Cx<R>(0, 0);
-    hop_dir<R, DAG, 0, PHM>(g, s, c, in, U, acc);
-    hop_dir<R, DAG, 1, PHM>(g, s, c, in, U, acc);
-    hop_dir<R, DAG, 2, PHM>(g, s, c, in, U, acc);
-    hop_dir<R, DAG, 3, PHM>(g, s, c, in, U, acc);
-    Cx<R> p[12];
-    in.load(s, p);
-    if constexpr (CLOVER) {
-      R a[36];
-      Cx<R> v[6], o[6];
-#pragma unroll
-      for (int blk = 0; blk < 2; blk++) {
-        A.load(blk, s, a);
-#pragma unroll
-        for (int k = 0; k < 6; k++) v[k] = p[6 * blk + k];
-        herm6_mul(a, v, o);
-#pragma unroll
-        for (int k = 0; k < 6; k++) out[6 * blk + k] = o[k] - kappa * acc[6 * blk + k];
-      }
-    } else {
-#pragma unroll
-      for (int k = 0; k < 12; k++) out[k] = p[k] - kappa * acc[k];
-    }
+    wilson_site_out<R, DAG, CLOVER, PHM>(g, s, c, in, U, A, kappa, out);
   }
   epi(s, active, out);
 }
+
 
 // ---------------------------------------------------------------------------
 // two sites per thread (FP32 arithmetic; see lmb_pair.cuh): lane x = site

@@ -39,7 +39,8 @@ EXPORTED = (
     "lmb_hisq_link_pullback", "lmb_hisq_fermion_force",
     "lmb_wilson_clover_link_pullback", "lmb_wilson_clover_fermion_force",
     "lmb_domainwall_set", "lmb_domainwall_apply", "lmb_solve_evenodd",
-    "lmb_set_halo", "lmb_operator_timing",
+    "lmb_set_halo", "lmb_operator_timing", "lmb_nccl_unique_id",
+    "lmb_set_process_grid",
 )
 
 
@@ -178,6 +179,9 @@ def load(path: str = LIB_PATH):
         lib.lmb_field_dot.argtypes = [vp, vp, vp, ctypes.c_int, dp, vp]
         lib.lmb_operator_timing.argtypes = [vp, ctypes.POINTER(CGParams), vp,
                                             ctypes.c_int, ctypes.c_int, dp, vp]
+        lib.lmb_nccl_unique_id.argtypes = [vp]
+        lib.lmb_set_process_grid.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int,
+                                             ip, ip, ctypes.c_uint, ip, ip]
         lib.lmb_random_su3_links.argtypes = [vp, ctypes.POINTER(vp),
                                              ctypes.c_double, ctypes.c_uint64,
                                              vp]
@@ -198,6 +202,17 @@ def require_cuda():
     import torch
     if not torch.cuda.is_available():
         raise LMBError("liblmb200 needs a CUDA device; none is visible")
+
+
+def nccl_unique_id() -> bytes:
+    """128 bytes naming a new NCCL communicator (ncclGetUniqueId, through
+    liblmb200's run-time NCCL)."""
+    lib = load()
+    buf = ctypes.create_string_buffer(128)
+    rc = lib.lmb_nccl_unique_id(buf)
+    if rc != LMB_OK:
+        raise LMBError(f"lmb_nccl_unique_id failed ({rc}): NCCL unavailable")
+    return buf.raw
 
 
 class Context:
@@ -242,6 +257,20 @@ class Context:
         self.check(self.lib.lmb_set_geometry(self.handle, Lc, int(nw), re, im,
                                              cc, int(dtype)))
         self._geom = key
+
+    def set_process_grid(self, nccl_id, nranks, rank, dims, coords, split,
+                         nb_minus, nb_plus):
+        """lmb_set_process_grid: this context's fields become the block of
+        `rank` in a process grid `dims` (NCCL communicator from the 128-byte
+        `nccl_id`); `split` lists the exchanged dimensions.  nccl_id None:
+        back to one lattice per context."""
+        iv = lambda v: (ctypes.c_int * 4)(*[int(x) for x in v])
+        mask = sum(1 << mu for mu in range(4) if split[mu])
+        idbuf = None if nccl_id is None else ctypes.create_string_buffer(bytes(nccl_id), 128)
+        self.check(self.lib.lmb_set_process_grid(
+            self.handle, idbuf, int(nranks), int(rank), iv(dims), iv(coords),
+            mask, iv(nb_minus), iv(nb_plus)))
+        self._geom = None
 
     def upload_links(self, which, ptrs, epochs, stream=None):
         arr = (ctypes.c_void_p * 4)(*ptrs)

@@ -145,3 +145,71 @@ def allreduce_complex(z, device):
     t = torch.tensor([complex(z).real, complex(z).imag], dtype=torch.float64, device=device)
     dist.all_reduce(t)
     return complex(float(t[0]), float(t[1]))
+
+
+# ---------------------------------------------------------------------------
+# the native sharded operators (lmb_set_process_grid)
+# ---------------------------------------------------------------------------
+def native_grid(ls) -> bool:
+    """True when the blocks of `ls` run the native sharded stencils: CUDA
+    fields of a 4-dimensional lattice on an NCCL process group.  (gloo
+    groups keep the exchange-then-compute path of the operators.)"""
+    if ls.dims == (1,) * ls.dim or ls.dim != 4 or not ls.A.is_cuda:
+        return False
+    return _dist().get_backend() == "nccl"
+
+
+def grid_arguments(ls):
+    """(dims, coords, split, nb_minus, nb_plus) of lmb_set_process_grid for
+    this rank's block of `ls`: the dimensions held by more than one rank are
+    split (faces exchanged with the Cartesian neighbours, exchange_dim!);
+    the others wrap inside the block with the boundary phase
+    (exchange_dim_local!)."""
+    split = tuple(int(p > 1) for p in ls.dims)
+    nbm, nbp = [], []
+    for d in range(4):
+        m, p = neighbours(ls, d)
+        nbm.append(m)
+        nbp.append(p)
+    return tuple(ls.dims), tuple(ls.coords), split, tuple(nbm), tuple(nbp)
+
+
+def shared_unique_id() -> bytes:
+    """An NCCL unique id made on rank 0 and broadcast to every rank of the
+    default group (a collective call)."""
+    from ._lib import nccl_unique_id
+    dist = _dist()
+    box = [nccl_unique_id() if dist.get_rank() == 0 else None]
+    dist.broadcast_object_list(box, src=0)
+    return box[0]
+
+
+def attach_process_grid(ctx, ls):
+    """Give context `ctx` the process grid of `ls` (collective on the first
+    call and whenever the grid changes; a no-op afterwards)."""
+    dist = _dist()
+    args = grid_arguments(ls)
+    key = (dist.get_world_size(), dist.get_rank()) + args
+    if getattr(ctx, "_grid_key", None) == key:
+        return
+    nid = shared_unique_id()
+    dims, coords, split, nbm, nbp = args
+    ctx.set_process_grid(nid, dist.get_world_size(), dist.get_rank(), dims,
+                         coords, split, nbm, nbp)
+    ctx._grid_key = key
+
+
+def bind_grid(ctx, psi, link_sets, stream):
+    """Bind the block of `psi` and the link sets [(which, links), ...] to a
+    context with the native process grid: the links' halos are filled first
+    (ensure_halo!, the ghost links of the backward hops come from them)."""
+    from .lattice import ensure_halo_
+    for _, links in link_sets:
+        for u in links:
+            ensure_halo_(u)
+    attach_process_grid(ctx, psi)
+    ctx.set_geometry(psi.PN, psi.nw, psi.phases, psi.coords, psi.dtype_code)
+    for which, links in link_sets:
+        ctx.upload_links(which, [u.data_ptr() for u in links],
+                         [u.halo_epoch.core for u in links], stream)
+    return ctx

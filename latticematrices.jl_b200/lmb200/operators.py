@@ -108,6 +108,9 @@ class _LinkOperator:
 
     def _bind(self, psi, stream):
         if psi.dims != (1,) * psi.dim:
+            from .distributed import bind_grid, native_grid
+            if native_grid(psi):   # NCCL: faces exchanged under the interior sites
+                return bind_grid(self.ctx, psi, [(LINKS_THIN, self.U)], stream)
             return self._bind_block(psi, stream)
         ctx = self.ctx
         ctx.set_geometry(psi.gsize, psi.nw, psi.phases, psi.coords,
@@ -298,9 +301,20 @@ def _validate_staggered_links(U, label="gauge link U"):
             raise ArgumentError(f"{label}[{mu}] must use periodic boundary phases")
 
 
-def _validate_staggered_application(result, links, psi, what="gauge link U"):
-    require_single_rank(psi)
-    """_validate_staggered_application (StaggeredDiracOperator.jl:66-92)."""
+def _validate_staggered_application(result, links, psi, what="gauge link U",
+                                    depth=1):
+    """_validate_staggered_application (StaggeredDiracOperator.jl:66-92).
+    A field split over a process grid runs on the native sharded stencils
+    (CUDA fields on an NCCL group) with links split the same way and a halo
+    of at least the stencil's reach `depth`; any other split field takes one
+    rank per lattice."""
+    from .distributed import native_grid
+    if not native_grid(psi):
+        require_single_rank(psi)
+    elif psi.nw < depth or any(link.dims != psi.dims for link in links):
+        raise ArgumentError(
+            f"a field split over a process grid needs links split the same "
+            f"way and nw >= {depth}")
     if result is psi:
         raise ArgumentError("staggered mul! requires distinct result and input fields")
     if not result.same_geometry(psi):
@@ -419,6 +433,11 @@ class HISQDiracOperator4D:
 
     def _bind(self, psi, stream):
         from ._lib import LINKS_FAT, LINKS_LONG
+        from .distributed import bind_grid, native_grid
+        if native_grid(psi):   # NCCL: three-layer faces under the interior sites
+            return bind_grid(self.ctx, psi,
+                             [(LINKS_FAT, self.links.fat_links),
+                              (LINKS_LONG, self.links.long_links)], stream)
         require_single_rank(psi)
         ctx = self.ctx
         ctx.set_geometry(psi.gsize, psi.nw, psi.phases, psi.coords,
@@ -432,7 +451,7 @@ class HISQDiracOperator4D:
     def _apply(self, out, psi, dagger, precision):
         _validate_staggered_application(
             out, self.links.fat_links + self.links.long_links, psi,
-            "fat link X")
+            "fat link X", depth=3)
         st = _stream()
         ctx = self._bind(psi, st)
         ctx.check(ctx.lib.lmb_hisq_apply(

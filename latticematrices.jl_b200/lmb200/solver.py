@@ -114,7 +114,7 @@ def cg_(x, A, b, r=None, p=None, Ap=None, *, rtol=1e-10, atol=0.0,
     if precision not in PREC:
         raise ArgumentError(f"unknown precision {precision!r}")
     native = _native_operator(A)
-    if native is not None and b.dims != (1,) * b.dim:
+    if native is not None and b.dims != (1,) * b.dim and not _grid_native(native[0], b):
         # fields split over a process grid: the reference's loop with
         # all-reduced dots, D applied per rank block (Wilson / clover only)
         if op_allows_blocks(native[0]) and precision == "double":
@@ -125,7 +125,8 @@ def cg_(x, A, b, r=None, p=None, Ap=None, *, rtol=1e-10, atol=0.0,
             "operators in FP64; other operators and mixed precision take one "
             "rank per lattice")
     if native is not None:
-        require_single_rank(b)
+        if not _grid_native(native[0], b):
+            require_single_rank(b)
         D, op = native
         binder = D.wilson if op == OP_WILSON_CLOVER else D
         prm = CGParams()
@@ -237,6 +238,20 @@ def solve_evenodd_(x, D, b, *, rtol=1e-10, atol=0.0, maxiter=5000,
                     res.reliable_updates, res.true_residual_norm,
                     res.dslash_ms, res.update_ms, res.dslash_launches,
                     res.update_launches, res.kernel_launches, res.link_reals)
+
+
+def _grid_native(D, b):
+    """A field split over a process grid whose D'D CG runs natively: CUDA
+    fields on an NCCL group, an operator with the sharded stencils (Wilson,
+    Wilson-clover, staggered, HISQ on given fat / long links); every
+    precision, the reductions summed over the ranks in the library."""
+    from .distributed import native_grid
+    from .hisq import HISQDiracCache4D
+    if isinstance(D, HISQDiracCache4D):
+        return False
+    return native_grid(b) and isinstance(
+        D, (WilsonDiracOperator4D, WilsonDiracCloverOperator4D,
+            StaggeredDiracOperator4D, HISQDiracOperator4D))
 
 
 def op_allows_blocks(D):
