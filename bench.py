@@ -740,12 +740,23 @@ def run_batched(args):
     clear()
     rs, t_seq = _timed(sequential, st)
     total_sites_rhs = sum(L[0] * L[1] * L[2] * L[3] * n for L, n in shapes)
+    # Algorithmic bytes of one CG iteration with every system running (FP32
+    # fields, reconstruct-12 FP32 links 192 B/site read once per group by K1
+    # and by K2): per site 2 x 192 per group of NB right-hand sides, and per
+    # right-hand side K1 p + tmp (192), K2 tmp + p + r rw + x rw (576), K3
+    # r + p rw (288).  Against the tuner's measured ms per such iteration.
+    nb = max(int(tune["rhs_block"]), 1)
+    it_bytes = sum(L[0] * L[1] * L[2] * L[3] * (384 * (-(-n // nb)) + 1056 * n) for L, n in shapes)
+    peak, peak_kind = measured_peak()
+    gbs = it_bytes / (tune["ms_per_iteration"] * 1e-3) / 1e9
     print(json.dumps({"workload": "batched Wilson D'D CG: " + " + ".join(
                           "%d^4 x%d" % (L[0], n) for L, n in shapes),
                       "batched_s": t_batch, "sequential_s": t_seq, "speedup": t_seq / t_batch,
                       "all_converged": all(r.converged for r in res),
                       "max_iterations": max(r.iterations for r in res),
-                      "tuning": tune, "site_rhs": total_sites_rhs}), flush=True)
+                      "tuning": tune, "site_rhs": total_sites_rhs,
+                      "roofline": {"bytes_per_iteration": it_bytes, "gbs": gbs, "peak_gbs": peak,
+                                   "peak_kind": peak_kind, "hbm_frac": gbs / peak}}), flush=True)
 
 
 def run_force(args):

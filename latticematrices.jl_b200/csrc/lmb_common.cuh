@@ -76,6 +76,13 @@ struct Geom {
   int eta_off[4];       // global coordinate of the local origin (staggered eta)
 };
 
+// the sites [lo, hi) of one stencil launch: the whole lattice, or the
+// interior slab of a block split along t only (every t-hop stays local)
+struct SiteRange {
+  int lo, hi;
+};
+inline SiteRange whole(const Geom &g) { return SiteRange{0, (int)g.V}; }
+
 LMB_D void site_coords(const Geom &g, int s, int c[4]) {
   int q = s / g.L[0];
   c[0] = s - q * g.L[0];

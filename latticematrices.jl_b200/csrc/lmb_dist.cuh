@@ -58,6 +58,13 @@ LMB_D bool dist_interior(const Geom &g, const DistView &dv, const int *c) {
   return true;
 }
 
+// the interior of a block split along t only as one range of sites,
+// t in [depth, L_t - depth); empty for any other split
+inline SiteRange t_slab(const Geom &g, const DistView &dv) {
+  if (dv.split != 8u || g.L[3] <= 2 * dv.depth) return SiteRange{0, 0};
+  return SiteRange{dv.depth * g.stride[3], (int)g.V - dv.depth * g.stride[3]};
+}
+
 // spinor at distance d (|d| <= depth) along MU from site s: a split
 // dimension reads a ghost layer past the block (*wrap = 0), any other
 // dimension wraps periodically (*wrap = signed number of edge crossings)
@@ -105,15 +112,24 @@ LMB_D void load_link_nb(const G &U, const GhostLinks<G> &gu, const Geom &g, cons
 }
 
 // ---------------------------------------------------------------------------
-// face packing: minus face (x_mu = j) -> send_m, plus face (x_mu = L-1-j) ->
-// send_p, each multiplied by its phase factor (1 unless the rank holds the
-// global edge)
+// face packing, every split dimension in one launch (blockIdx.y = the n-th
+// split dimension mu[n]): minus face (x_mu = j) -> send_m, plus face
+// (x_mu = L-1-j) -> send_p, each multiplied by its phase factor (1 unless
+// the rank holds the global edge)
 // ---------------------------------------------------------------------------
 template <int P, int NC>
+struct FacePack {
+  Field<P, NC> send_m[4], send_p[4];
+  double2 ph_m[4], ph_p[4];
+  int mu[4];
+};
+
+template <int P, int NC>
 __global__ void __launch_bounds__(256)
-    pack_faces_kernel(const Field<P, NC> in, Field<P, NC> send_m, Field<P, NC> send_p, const Geom g,
-                      const DistView dv, int mu, double2 ph_m, double2 ph_p) {
+    pack_faces_kernel(const Field<P, NC> in, const FacePack<P, NC> fp, const Geom g, const DistView dv) {
   typedef typename Real<P>::type R;
+  const int n = blockIdx.y;
+  const int mu = fp.mu[n];
   const int64_t F = dv.face[mu];
   const int64_t t = (int64_t)blockIdx.x * 256 + threadIdx.x;
   if (t >= dv.depth * F) return;
@@ -130,21 +146,22 @@ __global__ void __launch_bounds__(256)
   c[mu] = layer;
   int s = c[0] + g.stride[1] * c[1] + g.stride[2] * c[2] + g.stride[3] * c[3];
   in.load(s, v);
-  if (ph_m.x != 1.0 || ph_m.y != 0.0) {
-    const Cx<R> ph((R)ph_m.x, (R)ph_m.y);
+  const double2 pm = fp.ph_m[n], pp = fp.ph_p[n];
+  if (pm.x != 1.0 || pm.y != 0.0) {
+    const Cx<R> ph((R)pm.x, (R)pm.y);
 #pragma unroll
     for (int k = 0; k < NC; k++) v[k] = v[k] * ph;
   }
-  send_m.store(t, v);
+  fp.send_m[n].store(t, v);
   c[mu] = g.L[mu] - 1 - layer;
   s = c[0] + g.stride[1] * c[1] + g.stride[2] * c[2] + g.stride[3] * c[3];
   in.load(s, v);
-  if (ph_p.x != 1.0 || ph_p.y != 0.0) {
-    const Cx<R> ph((R)ph_p.x, (R)ph_p.y);
+  if (pp.x != 1.0 || pp.y != 0.0) {
+    const Cx<R> ph((R)pp.x, (R)pp.y);
 #pragma unroll
     for (int k = 0; k < NC; k++) v[k] = v[k] * ph;
   }
-  send_p.store(t, v);
+  fp.send_p[n].store(t, v);
 }
 
 // link ghost of dimension mu from the caller's padded links (halo filled):

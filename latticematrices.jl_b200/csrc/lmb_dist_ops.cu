@@ -1,7 +1,7 @@
-// lmb_dist_ops.cu -- the sharded path: process grid and NCCL communicator of a
-// context (lmb_set_process_grid), ghost links and boundary lists, the face
-// exchange's all-reduce, F_mu_nu of a block, and the drivers of the sharded
-// Wilson / Wilson-clover and staggered / HISQ operators.
+// lmb_dist_ops.cu -- the sharded path's host side: process grid and NCCL
+// communicator of a context (lmb_set_process_grid), ghost links and boundary
+// lists, the all-reduce of the partial sums and F_mu_nu of a block.  The
+// operator drivers are instantiated per precision in lmb_dist_{d,s,h}.cu.
 #include <dlfcn.h>
 
 #include "lmb_op_dist.cuh"
@@ -206,9 +206,6 @@ int dist_field_strength(lmb_ctx *ctx, cudaStream_t st) {
   LMB_CHECK_LAUNCH(ctx);
   return LMB_OK;
 }
-
-LMB_OP_INSTANCES(, DistWilsonPolicy)
-LMB_OP_INSTANCES(, DistStaggeredPolicy)
 
 }  // namespace lmb
 

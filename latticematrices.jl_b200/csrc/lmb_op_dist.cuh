@@ -19,6 +19,10 @@ int dist_exchange(lmb_ctx *ctx, const Field<P, NC> &in, const DistView &dv, Ghos
   const char *tag = P == PREC_DOUBLE ? "d" : (P == PREC_SINGLE ? "s" : "h");
   Field<P, NC> sm[4], sp[4];
   size_t span[4] = {0, 0, 0, 0};
+  FacePack<P, NC> fp{};
+  int nsplit = 0;
+  int64_t vmax = 0;
+  const Geom &g = ctx->g;
   for (int mu = 0; mu < 4; mu++) {
     if (!((dv.split >> mu) & 1)) continue;
     const int64_t Vg = (int64_t)dv.depth * dv.face[mu];
@@ -28,13 +32,19 @@ int dist_exchange(lmb_ctx *ctx, const Field<P, NC> &in, const DistView &dv, Ghos
       return fail(ctx, LMB_ERR_CUDA, "out of device memory (ghost buffers)");
     const size_t nb = Field<P, NC>::bytes(Vg), mb = Field<P, NC>::norm_bytes(Vg);
     span[mu] = mb ? ((nb + 255) / 256) * 256 + mb : nb;
-    const Geom &g = ctx->g;
     // the rank holding global coordinate 0 sends its minus face across the
     // edge (x phase); the one holding the last coordinate its plus face (/ phase)
     const double2 one = make_double2(1.0, 0.0);
-    const double2 pm = d->coords[mu] == 0 ? make_double2(g.ph_fwd[mu][0], g.ph_fwd[mu][1]) : one;
-    const double2 pp = d->coords[mu] == d->dims[mu] - 1 ? make_double2(g.ph_bwd[mu][0], g.ph_bwd[mu][1]) : one;
-    pack_faces_kernel<P, NC><<<grid_for(Vg, 256), 256, 0, st>>>(in, sm[mu], sp[mu], g, dv, mu, pm, pp);
+    fp.send_m[nsplit] = sm[mu];
+    fp.send_p[nsplit] = sp[mu];
+    fp.ph_m[nsplit] = d->coords[mu] == 0 ? make_double2(g.ph_fwd[mu][0], g.ph_fwd[mu][1]) : one;
+    fp.ph_p[nsplit] = d->coords[mu] == d->dims[mu] - 1 ? make_double2(g.ph_bwd[mu][0], g.ph_bwd[mu][1]) : one;
+    fp.mu[nsplit] = mu;
+    nsplit++;
+    if (Vg > vmax) vmax = Vg;
+  }
+  if (nsplit) {
+    pack_faces_kernel<P, NC><<<dim3(grid_for(vmax, 256), nsplit), 256, 0, st>>>(in, fp, g, dv);
     LMB_CHECK_LAUNCH(ctx);
   }
   LMB_CUDA(ctx, cudaEventRecord(d->ev_packed, st));
@@ -113,9 +123,17 @@ struct DistWilsonPolicy {
     typedef typename Real<P>::type R;
     const Geom g = ctx->g;
     const R kappa = (R)base.kappa;
+    const SiteRange slab = t_slab(g, dv);
     return dist_stencil(
         ctx, 1, epi, st,
         [&](const Epi &e) {
+          if (slab.hi > slab.lo) {  // split along t only: the single-lattice kernels on the slab
+            if (phase_mode_of(g.phase_mask) == PH_T)
+              launch_wilson_cl<P, P, CLOVER, PH_T, DAG>(ctx, in, U, A, base.kappa, e, st, slab);
+            else
+              launch_wilson_cl<P, P, CLOVER, PH_ANY, DAG>(ctx, in, U, A, base.kappa, e, st, slab);
+            return;
+          }
           wilson_interior_kernel<R, DAG, CLOVER, PH_ANY><<<grid_for(g.V, kDslashThreads), kDslashThreads, 0, st>>>(
               g, dv, in, U, A, kappa, e);
         },
@@ -171,9 +189,14 @@ struct DistStaggeredPolicy {
     const R mass = (R)base.mass;
     const R fc = (R)(DAG ? -0.5 : 0.5);
     const R lc = (R)(DAG ? (1.0 + base.eps) / 48.0 : -(1.0 + base.eps) / 48.0);
+    const SiteRange slab = t_slab(g, dv);
     return dist_stencil(
         ctx, depth(), epi, st,
         [&](const Epi &e) {
+          if (slab.hi > slab.lo) {  // split along t only: the single-lattice kernels on the slab
+            base.template launch_range<P, DAG>(ctx, in, e, st, slab);
+            return;
+          }
           staggered_interior_kernel<R, NAIK, PH_ANY><<<grid_for(g.V, kStagThreads), kStagThreads, 0, st>>>(
               g, dv, in, X, Lk, mass, fc, lc, e);
         },
@@ -217,6 +240,7 @@ inline int op_allreduce_sums(lmb_ctx *ctx, const DistStaggeredPolicy &, cudaStre
   return dist_allreduce_sums(ctx, st);
 }
 
+// instantiated once per precision in lmb_dist_d.cu, lmb_dist_s.cu, lmb_dist_h.cu
 LMB_OP_INSTANCES(extern, DistWilsonPolicy)
 LMB_OP_INSTANCES(extern, DistStaggeredPolicy)
 

@@ -23,18 +23,20 @@ struct StaggeredPolicy {
     if (!ctx->links[LMB_LINKS_THIN].valid) return fail(ctx, LMB_ERR_STATE, "gauge links have not been uploaded");
     return ensure_link_precision(ctx, ctx->links[LMB_LINKS_THIN], prec, st);
   }
+  // rg: the sites to compute (the whole lattice, or the interior slab of a
+  // block split along t)
   template <int P, int PHM, int DAG, class Epi>
-  void launch_phm(lmb_ctx *ctx, const Field<P, 3> &in, const Epi &epi, cudaStream_t st) const {
+  void launch_phm(lmb_ctx *ctx, const Field<P, 3> &in, const Epi &epi, cudaStream_t st, const SiteRange rg) const {
     typedef typename Real<P>::type R;
     const Geom &g = ctx->g;
-    const unsigned grid = grid_for(g.V, kStagThreads);
+    const unsigned grid = grid_for(rg.hi - rg.lo, kStagThreads);
     const R fc = (R)(DAG ? -0.5 : 0.5);
     const R lc = (R)(DAG ? (1.0 + eps) / 48.0 : -(1.0 + eps) / 48.0);
     if constexpr (P == PREC_SINGLE && PHM == PH_T) {
       // x-adjacent two-site kernel: even x extent, 18-real FP32 links
       const LinkSet &thin = ctx->links[LMB_LINKS_THIN];
       if (ctx->pair_sites && ctx->adj_sites && g.L[0] % 2 == 0 && (naik || !thin.recon(P))) {
-        const unsigned grid2 = grid_for(g.V / 2, kStagThreads);
+        const unsigned grid2 = grid_for((rg.hi - rg.lo) / 2, kStagThreads);
         if (naik) {
           const Gauge<P> X = gauge_view<P>(ctx->links[LMB_LINKS_FAT], g.V);
           const Gauge<P> Lk = gauge_view<P>(ctx->links[LMB_LINKS_LONG], g.V);
@@ -42,14 +44,14 @@ struct StaggeredPolicy {
             if (ctx->persistent) {
               auto kern = staggered_adj_persistent_kernel<true, Epi>;
               const unsigned g2 = std::min(grid2, resident_grid(ctx, kern));
-              kern<<<g2, kStagThreads, 0, st>>>(g, in, X, Lk, mass, fc, lc, epi, (int)grid2);
+              kern<<<g2, kStagThreads, 0, st>>>(g, in, X, Lk, mass, fc, lc, epi, (int)grid2, rg);
               return;
             }
           }
-          staggered_adj_kernel<true><<<grid2, kStagThreads, 0, st>>>(g, in, X, Lk, mass, fc, lc, epi);
+          staggered_adj_kernel<true><<<grid2, kStagThreads, 0, st>>>(g, in, X, Lk, mass, fc, lc, epi, rg);
         } else {
           const Gauge<P> X = gauge_view<P>(thin, g.V);
-          staggered_adj_kernel<false><<<grid2, kStagThreads, 0, st>>>(g, in, X, X, mass, fc, lc, epi);
+          staggered_adj_kernel<false><<<grid2, kStagThreads, 0, st>>>(g, in, X, X, mass, fc, lc, epi, rg);
         }
         return;
       }
@@ -61,32 +63,36 @@ struct StaggeredPolicy {
         if (ctx->persistent) {
           auto kern = staggered_persistent_kernel<R, true, PHM, Field<P, 3>, Gauge<P>, Gauge<P>, Epi>;
           const unsigned g2 = std::min(grid, resident_grid(ctx, kern));
-          kern<<<g2, kStagThreads, 0, st>>>(g, in, X, Lk, (R)mass, fc, lc, epi, (int)grid);
+          kern<<<g2, kStagThreads, 0, st>>>(g, in, X, Lk, (R)mass, fc, lc, epi, (int)grid, rg);
           return;
         }
       }
-      staggered_dslash_kernel<R, true, PHM><<<grid, kStagThreads, 0, st>>>(g, in, X, Lk, (R)mass, fc, lc, epi);
+      staggered_dslash_kernel<R, true, PHM><<<grid, kStagThreads, 0, st>>>(g, in, X, Lk, (R)mass, fc, lc, epi, rg);
     } else {
       const LinkSet &ls = ctx->links[LMB_LINKS_THIN];
       const NoLinks none{g.V};
       if (ls.recon(P))
         staggered_dslash_kernel<R, false, PHM><<<grid, kStagThreads, 0, st>>>(g, in, gauge12_view<P>(ls, g.V),
-                                                                               none, (R)mass, fc, lc, epi);
+                                                                               none, (R)mass, fc, lc, epi, rg);
       else
         staggered_dslash_kernel<R, false, PHM><<<grid, kStagThreads, 0, st>>>(g, in, gauge_view<P>(ls, g.V),
-                                                                               none, (R)mass, fc, lc, epi);
+                                                                               none, (R)mass, fc, lc, epi, rg);
     }
   }
   template <int P, int DAG, class Epi>
   int launch(lmb_ctx *ctx, const Field<P, 3> &in, const Epi &epi, cudaStream_t st) const {
     // PH_T needs at most one edge crossing per hop: every extent >= 3.  The
     // FP64 HISQ stencils measured faster on B200 with the branch form (PH_ANY).
+    return launch_range<P, DAG>(ctx, in, epi, st, whole(ctx->g));
+  }
+  template <int P, int DAG, class Epi>
+  int launch_range(lmb_ctx *ctx, const Field<P, 3> &in, const Epi &epi, cudaStream_t st, const SiteRange rg) const {
     const int *L = ctx->g.L;
     if (P != PREC_DOUBLE && phase_mode_of(ctx->g.phase_mask) == PH_T && L[0] >= 3 && L[1] >= 3 && L[2] >= 3 &&
         L[3] >= 3)
-      launch_phm<P, PH_T, DAG>(ctx, in, epi, st);
+      launch_phm<P, PH_T, DAG>(ctx, in, epi, st, rg);
     else
-      launch_phm<P, PH_ANY, DAG>(ctx, in, epi, st);
+      launch_phm<P, PH_ANY, DAG>(ctx, in, epi, st, rg);
     LMB_CHECK_LAUNCH(ctx);
     return LMB_OK;
   }

@@ -8,44 +8,49 @@ namespace lmb {
 // ---------------------------------------------------------------------------
 // stencil launch (DAG: 0 = D, 1 = D^+)
 // ---------------------------------------------------------------------------
+// rg: the sites to compute (the whole lattice, or the interior slab of a
+// block split along t, whose pairs of x-adjacent sites it keeps whole)
 template <int PS, int PG, bool CLOVER, int PHM, int DAG, class G, class CL, class Epi>
 void launch_wilson_cl(lmb_ctx *ctx, const Field<PS, 12> &in, const G &U, const CL &A, double kappa,
-                      const Epi &epi, cudaStream_t st) {
+                      const Epi &epi, cudaStream_t st, const SiteRange rg) {
   typedef typename Real<PS>::type R;
   const Geom &g = ctx->g;
+  const bool all = rg.lo == 0 && rg.hi == (int)g.V;
   if constexpr (PS == PREC_HALF && std::is_same<G, Gauge12<PREC_HALF>>::value) {
     if (ctx->pair_sites && ctx->adj_sites && g.L[0] % 2 == 0) {
-      const unsigned ntiles = grid_for(g.V / 2, kDslashThreads);
+      const unsigned ntiles = grid_for((rg.hi - rg.lo) / 2, kDslashThreads);
       if constexpr (PersistentEpi<Epi>::value) {
         if (ctx->persistent) {
           auto kern = wilson_half_adj_persistent_kernel<DAG, CLOVER, PHM, CL, Epi>;
           const unsigned grid = std::min(ntiles, resident_grid(ctx, kern));
-          kern<<<grid, kDslashThreads, 0, st>>>(g, in, U, A, (float)kappa, epi, (int)ntiles);
+          kern<<<grid, kDslashThreads, 0, st>>>(g, in, U, A, (float)kappa, epi, (int)ntiles, rg);
           return;
         }
       }
-      wilson_half_adj_kernel<DAG, CLOVER, PHM><<<ntiles, kDslashThreads, 0, st>>>(g, in, U, A, (float)kappa, epi);
+      wilson_half_adj_kernel<DAG, CLOVER, PHM><<<ntiles, kDslashThreads, 0, st>>>(g, in, U, A, (float)kappa, epi,
+                                                                                   rg);
       return;
     }
   }
   if constexpr (PS != PREC_DOUBLE) {
-    if (ctx->pair_sites && g.L[3] % 2 == 0) {
+    if (all && ctx->pair_sites && g.L[3] % 2 == 0) {  // pairs (t, t + T/2): the whole lattice only
       wilson_dslash_pair_kernel<DAG, CLOVER, PHM><<<grid_for(g.V / 2, kDslashThreads), kDslashThreads, 0, st>>>(
           g, in, U, A, (float)kappa, epi);
       return;
     }
   }
-  wilson_dslash_kernel<R, DAG, CLOVER, PHM><<<grid_for(g.V, kDslashThreads), kDslashThreads, 0, st>>>(
-      g, in, U, A, (R)kappa, epi);
+  wilson_dslash_kernel<R, DAG, CLOVER, PHM><<<grid_for(rg.hi - rg.lo, kDslashThreads), kDslashThreads, 0, st>>>(
+      g, in, U, A, (R)kappa, epi, rg);
 }
 
 template <int PS, int PG, bool CLOVER, int PHM, int DAG, class G, class Epi>
 void launch_wilson_phm(lmb_ctx *ctx, const Field<PS, 12> &in, const G &U, double kappa, const Epi &epi,
                        cudaStream_t st) {
   if constexpr (CLOVER)
-    launch_wilson_cl<PS, PG, true, PHM, DAG>(ctx, in, U, clover_view<PG>(ctx->clover, ctx->g.V), kappa, epi, st);
+    launch_wilson_cl<PS, PG, true, PHM, DAG>(ctx, in, U, clover_view<PG>(ctx->clover, ctx->g.V), kappa, epi, st,
+                                             whole(ctx->g));
   else
-    launch_wilson_cl<PS, PG, false, PHM, DAG>(ctx, in, U, NoClover{ctx->g.V}, kappa, epi, st);
+    launch_wilson_cl<PS, PG, false, PHM, DAG>(ctx, in, U, NoClover{ctx->g.V}, kappa, epi, st, whole(ctx->g));
 }
 
 template <int PS, int PG, bool CLOVER, int DAG, class G, class Epi>

@@ -179,7 +179,10 @@ struct EpiStoreNorm {  // K1
   }
   LMB_D void finish(double (&red)[1]) const {
     double tot[1];
-    if (grid_reduce<kDslashThreads, 1>(red, partials, counter, tot) && threadIdx.x == 0) finalize_pAp(st, tot[0]);
+    if (grid_reduce<kDslashThreads, 1>(red, partials, counter, tot) && threadIdx.x == 0) {
+      if (local) *local = tot[0];
+      else finalize_pAp(st, tot[0]);
+    }
   }
   LMB_D void pair(int s0, int s1, bool active, const Cx2 *v) const {
     double n2[1] = {0.0}, tot[1];
@@ -190,8 +193,10 @@ struct EpiStoreNorm {  // K1
       for (int k = 0; k < NC; k++) q = norm2_acc(v[k], q);
       n2[0] = (double)q.x + (double)q.y;
     }
-    if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0)
-      finalize_pAp(st, tot[0]);
+    if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0) {
+      if (local) *local = tot[0];
+      else finalize_pAp(st, tot[0]);
+    }
   }
 };
 
@@ -255,7 +260,10 @@ struct EpiCGUpdate {  // K2
   }
   LMB_D void finish(double (&red)[1]) const {
     double tot[1];
-    if (grid_reduce<kDslashThreads, 1>(red, partials, counter, tot) && threadIdx.x == 0) finalize_rr(st, tot[0]);
+    if (grid_reduce<kDslashThreads, 1>(red, partials, counter, tot) && threadIdx.x == 0) {
+      if (local) *local = tot[0];
+      else finalize_rr(st, tot[0]);
+    }
   }
   LMB_D void pair(int s0, int s1, bool active, const Cx2 *v) const {
     double n2[1] = {0.0}, tot[1];
@@ -277,8 +285,10 @@ struct EpiCGUpdate {  // K2
       store2(x, s0, s1, xv);
       n2[0] = (double)q.x + (double)q.y;
     }
-    if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0)
-      finalize_rr(st, tot[0]);
+    if (grid_reduce<kDslashThreads, 1>(n2, partials, counter, tot) && threadIdx.x == 0) {
+      if (local) *local = tot[0];
+      else finalize_rr(st, tot[0]);
+    }
   }
 };
 

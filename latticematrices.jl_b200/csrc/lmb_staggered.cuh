@@ -185,10 +185,10 @@ template <int NC> struct StagMinBlocks<double, EpiCGUpdate<PREC_DOUBLE, PREC_DOU
 template <typename R, bool NAIK, int PHM, class SF, class GF, class GL, class Epi>
 __global__ void __launch_bounds__(kStagThreads, (StagMinBlocks<R, Epi>::value))
     staggered_dslash_kernel(const Geom g, const SF in, const GF X, const GL Lk, const R mass, const R fc,
-                            const R lc, Epi epi) {
+                            const R lc, Epi epi, const SiteRange rg) {
   if (epi.skip()) return;
-  const int s = blockIdx.x * kStagThreads + threadIdx.x;
-  const bool active = s < g.V;
+  const int s = rg.lo + blockIdx.x * kStagThreads + threadIdx.x;
+  const bool active = s < rg.hi;
   Cx<R> out[3];
   if (active) stag_site<R, NAIK, PHM>(g, s, in, X, Lk, mass, fc, lc, out);
   epi(s, active, out);
@@ -200,12 +200,12 @@ __global__ void __launch_bounds__(kStagThreads, (StagMinBlocks<R, Epi>::value))
 template <typename R, bool NAIK, int PHM, class SF, class GF, class GL, class Epi>
 __global__ void __launch_bounds__(kStagThreads, LMB_STAG_PMINB)
     staggered_persistent_kernel(const Geom g, const SF in, const GF X, const GL Lk, const R mass, const R fc,
-                                const R lc, Epi epi, int ntiles) {
+                                const R lc, Epi epi, int ntiles, const SiteRange rg) {
   if (epi.skip()) return;
   double red[1] = {0.0};
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int s = tile * kStagThreads + threadIdx.x;
-    const bool active = s < g.V;
+    const int s = rg.lo + tile * kStagThreads + threadIdx.x;
+    const bool active = s < rg.hi;
     Cx<R> out[3];
     if (active) stag_site<R, NAIK, PHM>(g, s, in, X, Lk, mass, fc, lc, out);
     epi.site_acc(s, active, out, red);
@@ -313,15 +313,17 @@ LMB_D void stag_adj_sites(const Geom &g, int s0, const Field<PREC_SINGLE, 3> &in
   }
 }
 
-// V/2 threads.  Epi must provide skip() and pair_adj(s0, active, out[3]).
+// one thread per pair of the range (rg.lo, rg.hi even).  Epi must provide
+// skip() and pair_adj(s0, active, out[3]).
 template <bool NAIK, class Epi>
 __global__ void __launch_bounds__(kStagThreads, LMB_PAIR_MINB)
     staggered_adj_kernel(const Geom g, const Field<PREC_SINGLE, 3> in, const Gauge<PREC_SINGLE> X,
-                         const Gauge<PREC_SINGLE> Lk, const float mass, const float fc, const float lc, Epi epi) {
+                         const Gauge<PREC_SINGLE> Lk, const float mass, const float fc, const float lc, Epi epi,
+                         const SiteRange rg) {
   if (epi.skip()) return;
   const int i = blockIdx.x * kStagThreads + threadIdx.x;
-  const bool active = i < (int)(g.V >> 1);
-  const int s0 = 2 * i;
+  const bool active = i < ((rg.hi - rg.lo) >> 1);
+  const int s0 = rg.lo + 2 * i;
   Cx2 out[3];
   if (active) stag_adj_sites<NAIK>(g, s0, in, X, Lk, mass, fc, lc, out);
   epi.pair_adj(s0, active, out);
@@ -332,14 +334,14 @@ template <bool NAIK, class Epi>
 __global__ void __launch_bounds__(kStagThreads, LMB_PAIR_MINB)
     staggered_adj_persistent_kernel(const Geom g, const Field<PREC_SINGLE, 3> in, const Gauge<PREC_SINGLE> X,
                                     const Gauge<PREC_SINGLE> Lk, const float mass, const float fc, const float lc,
-                                    Epi epi, int ntiles) {
+                                    Epi epi, int ntiles, const SiteRange rg) {
   if (epi.skip()) return;
   double red[1] = {0.0};
-  const int npairs = (int)(g.V >> 1);
+  const int npairs = (rg.hi - rg.lo) >> 1;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int i = tile * kStagThreads + threadIdx.x;
     const bool active = i < npairs;
-    const int s0 = 2 * i;
+    const int s0 = rg.lo + 2 * i;
     Cx2 out[3];
     if (active) stag_adj_sites<NAIK>(g, s0, in, X, Lk, mass, fc, lc, out);
     epi.pair_adj_acc(s0, active, out, red);

@@ -255,10 +255,10 @@ LMB_D void wilson_site_out(const Geom &g, int s, const int *c, const SF &in, con
 template <typename R, int DAG, bool CLOVER, int PHM, class SF, class G, class CL, class Epi>
 __global__ void __launch_bounds__(kDslashThreads, LMB_DSLASH_MINB)
     wilson_dslash_kernel(const Geom g, const SF in, const G U, const CL A,
-                         const R kappa, Epi epi) {
+                         const R kappa, Epi epi, const SiteRange rg) {
   if (epi.skip()) return;
-  const int s = blockIdx.x * kDslashThreads + threadIdx.x;
-  const bool active = s < g.V;
+  const int s = rg.lo + blockIdx.x * kDslashThreads + threadIdx.x;
+  const bool active = s < rg.hi;
   Cx<R> out[12];
   if (active) {
     int c[4];
@@ -520,16 +520,16 @@ LMB_D void half_adj_sites(const Geom &g, int s0, const Field<PREC_HALF, 12> &in,
   }
 }
 
-// V/2 threads; needs x even.  Epi must provide skip() and
-// pair_adj(s0, active, out[12]) (sites s0 and s0 + 1).
+// one thread per pair of the range (rg.lo, rg.hi even); needs x even.  Epi
+// must provide skip() and pair_adj(s0, active, out[12]) (sites s0, s0 + 1).
 template <int DAG, bool CLOVER, int PHM, class CL, class Epi>
 __global__ void __launch_bounds__(kDslashThreads, LMB_PAIR_MINB)
     wilson_half_adj_kernel(const Geom g, const Field<PREC_HALF, 12> in, const Gauge12<PREC_HALF> U, const CL A,
-                           const float kappa, Epi epi) {
+                           const float kappa, Epi epi, const SiteRange rg) {
   if (epi.skip()) return;
   const int i = blockIdx.x * kDslashThreads + threadIdx.x;
-  const bool active = i < (int)(g.V >> 1);
-  const int s0 = 2 * i;
+  const bool active = i < ((rg.hi - rg.lo) >> 1);
+  const int s0 = rg.lo + 2 * i;
   Cx2 out[12];
   if (active) half_adj_sites<DAG, CLOVER, PHM>(g, s0, in, U, A, kappa, out);
   epi.pair_adj(s0, active, out);
@@ -545,14 +545,14 @@ __global__ void __launch_bounds__(kDslashThreads, LMB_PAIR_MINB)
 template <int DAG, bool CLOVER, int PHM, class CL, class Epi>
 __global__ void __launch_bounds__(kDslashThreads, LMB_PAIR_MINB)
     wilson_half_adj_persistent_kernel(const Geom g, const Field<PREC_HALF, 12> in, const Gauge12<PREC_HALF> U,
-                                      const CL A, const float kappa, Epi epi, int ntiles) {
+                                      const CL A, const float kappa, Epi epi, int ntiles, const SiteRange rg) {
   if (epi.skip()) return;
   double red[1] = {0.0};
-  const int npairs = (int)(g.V >> 1);
+  const int npairs = (rg.hi - rg.lo) >> 1;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int i = tile * kDslashThreads + threadIdx.x;
     const bool active = i < npairs;
-    const int s0 = 2 * i;
+    const int s0 = rg.lo + 2 * i;
     Cx2 out[12];
     if (active) half_adj_sites<DAG, CLOVER, PHM>(g, s0, in, U, A, kappa, out);
     epi.pair_adj_acc(s0, active, out, red);

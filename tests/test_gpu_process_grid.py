@@ -5,7 +5,10 @@ phases of the global edge, NCCL send / receive into ghost buffers on the
 communication stream, the interior kernel, the ghost-aware boundary kernel,
 link ghosts from the caller's halo, the all-reduce of every CG reduction --
 and the result must equal the whole-lattice operator and the oracle
-(FP64 <= 1e-13, FP32 storage 5e-6, int16 storage 2e-3)."""
+(FP64 <= 1e-13, FP32 storage 5e-6, int16 storage 2e-3).  A block split
+along t only runs its interior slab on the single-lattice kernels (int16
+x-adjacent pairs, persistent reductions); other splits on the one-site
+interior kernel."""
 import ctypes
 
 import numpy as np
@@ -51,7 +54,7 @@ def _stream():
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
-@pytest.mark.parametrize("split", [(1, 0, 0, 1), (1, 1, 1, 1), (0, 1, 0, 0)])
+@pytest.mark.parametrize("split", [(1, 0, 0, 1), (1, 1, 1, 1), (0, 1, 0, 0), (0, 0, 0, 1)])
 @pytest.mark.parametrize("clover", [False, True])
 def test_wilson_on_a_split_block_matches_oracle(lmb, orc, split, clover):
     L, kappa, csw = (4, 6, 4, 8), 0.1355, 1.0
@@ -94,19 +97,20 @@ def _cg(lmb, ctx, op, x, b, prec, **kw):
     return res
 
 
+@pytest.mark.parametrize("split", [(1, 0, 1, 1), (0, 0, 0, 1)])
 @pytest.mark.parametrize("prec", ["double", "single", "half"])
-def test_clover_cg_on_a_split_block(lmb, orc, prec):
+def test_clover_cg_on_a_split_block(lmb, orc, prec, split):
     L, kappa, csw = (4, 4, 6, 8), 0.1355, 1.0
     U = orc.random_su3_links(L, 0.2, 3)
     b = orc.gaussian_field(L, 3, 4, 4)
     Ud = _links(lmb, U, 1)
     bd = lmb.LatticeMatrix.from_array(b, nw=1, phases=PHASES)
-    ctx = _grid_ctx(lmb, L, 1, PHASES, (1, 0, 1, 1))
+    ctx = _grid_ctx(lmb, L, 1, PHASES, split)
     st = _stream()
     ctx.upload_links(0, [u.data_ptr() for u in Ud], [u.halo_epoch.core for u in Ud], st)
     x = bd.similar()
     res = _cg(lmb, ctx, 1, x, bd, prec, kappa=kappa, csw=csw)
-    assert res.converged and res.reason == 0, (prec, res.iterations)
+    assert res.converged and res.reason == 0, (prec, split, res.iterations)
     op = orc.Operator(orc.OP_CLOVER, U, L, kappa=kappa, csw=csw, F=orc.clover_field_strength(U))
     xs = x.gather_matrix()
     true_rel = np.linalg.norm(b - op.ddagd(xs)) / np.linalg.norm(b)
@@ -116,29 +120,32 @@ def test_clover_cg_on_a_split_block(lmb, orc, prec):
         assert abs(res.iterations - ref["iterations"]) <= 1, (res.iterations, ref["iterations"])
 
 
-@pytest.mark.parametrize("split", [(1, 1, 1, 1), (0, 0, 1, 1)])
-def test_hisq_on_a_split_block_matches_oracle(lmb, orc, split):
-    L, mass, eps = (6, 4, 6, 6), 0.05, -0.083
+@pytest.mark.parametrize("split,L,phases", [((1, 1, 1, 1), (6, 4, 6, 6), TWISTED),
+                                            ((0, 0, 1, 1), (6, 4, 6, 6), TWISTED),
+                                            ((0, 0, 0, 1), (4, 4, 4, 8), TWISTED),
+                                            ((0, 0, 0, 1), (4, 4, 4, 8), PHASES)])
+def test_hisq_on_a_split_block_matches_oracle(lmb, orc, split, L, phases):
+    mass, eps = 0.05, -0.083
     U = orc.random_su3_links(L, 0.25, 5)
     X, Ln = orc.hisq_links_from_thin(U, eps)
     psi = orc.gaussian_field(L, 3, 1, 6)
     Xd, Ld = _links(lmb, X, 3), _links(lmb, Ln, 3)
-    pd = lmb.LatticeMatrix.from_array(psi, nw=3, phases=TWISTED)
-    ctx = _grid_ctx(lmb, L, 3, TWISTED, split)
+    pd = lmb.LatticeMatrix.from_array(psi, nw=3, phases=phases)
+    ctx = _grid_ctx(lmb, L, 3, phases, split)
     st = _stream()
     ctx.upload_links(1, [u.data_ptr() for u in Xd], [u.halo_epoch.core for u in Xd], st)
     ctx.upload_links(2, [u.data_ptr() for u in Ld], [u.halo_epoch.core for u in Ld], st)
     out = pd.similar()
     for dag in (0, 1):
-        ref = orc.hisq(X, Ln, psi, mass, eps, TWISTED, dagger=bool(dag))
+        ref = orc.hisq(X, Ln, psi, mass, eps, phases, dagger=bool(dag))
         for prec, tol in (("double", 1e-13), ("single", 5e-6), ("half", 2e-3)):
             ctx.check(ctx.lib.lmb_hisq_apply(ctx.handle, out.data_ptr(), pd.data_ptr(), mass, eps, dag,
                                              PREC[prec], st))
             err = rd.rel_err(out.gather_matrix(), ref)
             assert err <= tol, (split, dag, prec, err)
     # and the CG on the block, FP64 and FP32 inner iterations
-    bd = lmb.LatticeMatrix.from_array(psi, nw=3, phases=TWISTED)
-    op = orc.Operator(orc.OP_HISQ, list(X) + list(Ln), L, phases=TWISTED, mass=mass, naik_epsilon=eps)
+    bd = lmb.LatticeMatrix.from_array(psi, nw=3, phases=phases)
+    op = orc.Operator(orc.OP_HISQ, list(X) + list(Ln), L, phases=phases, mass=mass, naik_epsilon=eps)
     for prec in ("double", "single"):
         x = bd.similar()
         res = _cg(lmb, ctx, 3, x, bd, prec, mass=mass, eps=eps)
@@ -148,13 +155,14 @@ def test_hisq_on_a_split_block_matches_oracle(lmb, orc, split):
         assert true_rel <= 1.05e-10, (prec, true_rel)
 
 
-def test_staggered_on_a_split_block_matches_oracle(lmb, orc):
+@pytest.mark.parametrize("split", [(0, 1, 1, 0), (0, 0, 0, 1)])
+def test_staggered_on_a_split_block_matches_oracle(lmb, orc, split):
     L, mass = (4, 6, 4, 4), 0.07
     U = orc.random_su3_links(L, 0.3, 7)
     psi = orc.gaussian_field(L, 3, 1, 8)
     Ud = _links(lmb, U, 1)
     pd = lmb.LatticeMatrix.from_array(psi, nw=1, phases=TWISTED)
-    ctx = _grid_ctx(lmb, L, 1, TWISTED, (0, 1, 1, 0))
+    ctx = _grid_ctx(lmb, L, 1, TWISTED, split)
     st = _stream()
     ctx.upload_links(0, [u.data_ptr() for u in Ud], [u.halo_epoch.core for u in Ud], st)
     out = pd.similar()
