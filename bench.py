@@ -699,8 +699,10 @@ def run_hisq_dslash(args):
 def run_batched(args):
     """16 Gaussian right-hand sides of Wilson D'D on 32^4 plus
     lattices 8^4 x4, 12^4 x4, 16^4 x2, 24^4 x1, in one batched solve (FP32
-    inner, FP64 reliable updates, CUDA graph, autotuned); compared with
-    solving the same systems one right-hand side at a time."""
+    arithmetic on FP32 or int16 iterated fields, FP64 reliable updates, CUDA
+    graph, autotuned kernel family / group size / tile); compared with
+    solving the same systems one right-hand side at a time with the
+    single-lattice kernels at the same storage precision."""
     import torch
     import lmb200 as lmb
     shapes = [((32, 32, 32, 32), 16), ((8, 8, 8, 8), 4), ((12, 12, 12, 12), 4),
@@ -717,46 +719,56 @@ def run_batched(args):
             pairs.append((b.similar(), b))
         systems.append((D, pairs))
     st = torch.cuda.current_stream()
+    peak, peak_kind = measured_peak()
+    rb = {"single": 96, "half": 52}     # bytes of one stored Wilson spinor (int16: + norm)
 
     def clear():
         for _, pairs in systems:
             for x, _ in pairs:
                 lmb.clear_matrix_(x)
 
-    clear()
-    lmb.cg_batched_(systems, rtol=1e-10)          # tuning + warm-up
-    clear()
-    (res, tune), t_batch = _timed(lambda: lmb.cg_batched_(systems, rtol=1e-10), st)
-    # one right-hand side at a time, same kernels' single-system path
-    def sequential():
-        rs = []
-        for D, pairs in systems:
-            A = lmb.DdagDOp(D, pairs[0][1].similar())
-            for x, b in pairs:
-                rs.append(lmb.cg_(x, A, b, rtol=1e-10, precision="single"))
-        return rs
-    clear()
-    sequential()
-    clear()
-    rs, t_seq = _timed(sequential, st)
+    out = {}
+    for prec in ("single", "half"):
+        clear()
+        lmb.cg_batched_(systems, rtol=1e-10, precision=prec)          # tuning + warm-up
+        clear()
+        (res, tune), t_batch = _timed(lambda: lmb.cg_batched_(systems, rtol=1e-10, precision=prec), st)
+
+        def sequential():
+            rs = []
+            for D, pairs in systems:
+                A = lmb.DdagDOp(D, pairs[0][1].similar())
+                for x, b in pairs:
+                    rs.append(lmb.cg_(x, A, b, rtol=1e-10, precision=prec))
+            return rs
+        clear()
+        sequential()
+        clear()
+        rs, t_seq = _timed(sequential, st)
+        # Algorithmic bytes of the two stencil stages of one CG iteration with
+        # every system running, what the tuner's ms_stencils times: the
+        # reconstruct-12 FP32 links (192 B/site) once per group of NB
+        # right-hand sides by each stage, and per right-hand side K1 p + tmp,
+        # K2 tmp + p + r rw (spinors S) + x_low rw (FP32, 96 B).
+        nb = max(int(tune["rhs_block"]), 1)
+        S = rb[prec]
+        k12 = sum(L[0] * L[1] * L[2] * L[3] * (384 * (-(-n // nb)) + (6 * S + 192) * n) for L, n in shapes)
+        gbs = k12 / (tune["ms_stencils"] * 1e-3) / 1e9
+        out[prec] = {"batched_s": t_batch, "sequential_s": t_seq, "speedup": t_seq / t_batch,
+                     "all_converged": all(r.converged for r in res),
+                     "sequential_converged": all(r.converged for r in rs),
+                     "max_iterations": max(r.iterations for r in res),
+                     "max_rel_residual": max(r.relative_residual for r in res),
+                     "tuning": tune,
+                     "roofline": {"kernels": "K1 + K2 of one iteration, every system running",
+                                  "bytes": k12, "gbs": gbs, "peak_gbs": peak, "peak_kind": peak_kind,
+                                  "hbm_frac": gbs / peak}}
     total_sites_rhs = sum(L[0] * L[1] * L[2] * L[3] * n for L, n in shapes)
-    # Algorithmic bytes of one CG iteration with every system running (FP32
-    # fields, reconstruct-12 FP32 links 192 B/site read once per group by K1
-    # and by K2): per site 2 x 192 per group of NB right-hand sides, and per
-    # right-hand side K1 p + tmp (192), K2 tmp + p + r rw + x rw (576), K3
-    # r + p rw (288).  Against the tuner's measured ms per such iteration.
-    nb = max(int(tune["rhs_block"]), 1)
-    it_bytes = sum(L[0] * L[1] * L[2] * L[3] * (384 * (-(-n // nb)) + 1056 * n) for L, n in shapes)
-    peak, peak_kind = measured_peak()
-    gbs = it_bytes / (tune["ms_per_iteration"] * 1e-3) / 1e9
     print(json.dumps({"workload": "batched Wilson D'D CG: " + " + ".join(
                           "%d^4 x%d" % (L[0], n) for L, n in shapes),
-                      "batched_s": t_batch, "sequential_s": t_seq, "speedup": t_seq / t_batch,
-                      "all_converged": all(r.converged for r in res),
-                      "max_iterations": max(r.iterations for r in res),
-                      "tuning": tune, "site_rhs": total_sites_rhs,
-                      "roofline": {"bytes_per_iteration": it_bytes, "gbs": gbs, "peak_gbs": peak,
-                                   "peak_kind": peak_kind, "hbm_frac": gbs / peak}}), flush=True)
+                      "site_rhs": total_sites_rhs, **out,
+                      "speedup_half_batched_vs_single_sequential":
+                          out["single"]["sequential_s"] / out["half"]["batched_s"]}), flush=True)
 
 
 def run_force(args):

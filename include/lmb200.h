@@ -305,8 +305,13 @@ typedef struct {
 typedef struct {
   int rhs_block;            /* right-hand sides sharing each link load */
   int threads;              /* sites per block */
-  double ms_per_iteration;  /* device time of one batched CG iteration */
+  double ms_per_iteration;  /* device time of one batched CG iteration
+                               (K1 + K2 + K3, averaged over the replays) */
   int graph_iterations;     /* iterations replayed from the CUDA graph */
+  int kernel_family;        /* 0: links in registers (rhs_block <= 4);
+                               1: links staged in shared memory (up to 16) */
+  double ms_stencils;       /* tuner's K1 + K2 time of one iteration with
+                               every system running */
 } lmb_batch_tuning;
 
 int lmb_cg_ddagd_batched(lmb_ctx *ctx, const lmb_cg_params *params,

@@ -285,6 +285,7 @@ lmb_ctx *lmb_create(int device) {
   if (const char *as = getenv("LMB_ADJ_SITES")) ctx->adj_sites = atoi(as) != 0;
   if (const char *dw = getenv("LMB_DW_TWO_PASS")) ctx->dw_two_pass = atoi(dw) != 0;
   if (const char *pe = getenv("LMB_PERSISTENT")) ctx->persistent = atoi(pe) != 0;
+  if (const char *bf = getenv("LMB_BATCH_FAMILY")) ctx->batch_family = atoi(bf);
   if (cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
     delete ctx;
     return nullptr;

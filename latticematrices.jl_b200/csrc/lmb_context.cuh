@@ -69,10 +69,14 @@ struct lmb_batch_links {
   int64_t V = 0;
   double2 *d12 = nullptr;  // FP64 reconstruct-12
   float4 *f12 = nullptr;   // FP32 reconstruct-12
+  int4 *h12 = nullptr;     // int16 reconstruct-12
 };
 
 struct lmb_batch_tune {
   int nb = 0, nt = 0;
+  // 0: links in registers, NB <= 4; 1: links in shared memory, NB up to 16;
+  // 2: int16 x-adjacent pairs, tasks (tile, member) sharing links through L2
+  int family = 0;
   double ms = 0;
 };
 
@@ -99,6 +103,9 @@ struct lmb_ctx {
   // slot walking the tiles, one reduction per block); LMB_PERSISTENT=0 in
   // the environment: one block per tile
   bool persistent = true;
+  // batched CG kernel family the autotuner may pick: -1 either, 0 links in
+  // registers, 1 links in shared memory (environment LMB_BATCH_FAMILY)
+  int batch_family = -1;
   int sm_count = 0;
   lmb::LinkSet links[3];
   // domain-wall operator (lmb_domainwall_set): L5 slices of the 4D geometry,

@@ -96,6 +96,8 @@ class BatchTuning(ctypes.Structure):
         ("rhs_block", ctypes.c_int), ("threads", ctypes.c_int),
         ("ms_per_iteration", ctypes.c_double),
         ("graph_iterations", ctypes.c_int),
+        ("kernel_family", ctypes.c_int),
+        ("ms_stencils", ctypes.c_double),
     ]
 
 

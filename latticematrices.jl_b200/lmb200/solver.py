@@ -369,12 +369,14 @@ def cg_batched_(systems, *, rtol=1e-10, atol=0.0, maxiter=5000, delta=0.1,
                 check_interval=0, precision="single"):
     """Solve D'D x = b for every (x, b) of every system in one batched CG
     (lmb_cg_ddagd_batched): systems = [(WilsonDiracOperator4D, [(x, b), ...]),
-    ...], lattices of any sizes.  FP32 inner iterations with FP64 reliable
-    updates; each right-hand side stops on its own FP64 true residual.
-    Returns (list of CGResult per right-hand side, tuning dict)."""
+    ...], lattices of any sizes.  FP32 arithmetic on FP32 (precision="single")
+    or int16 (precision="half") iterated fields with FP64 reliable updates;
+    each right-hand side stops on its own FP64 true residual.  Returns (list
+    of CGResult per right-hand side, tuning dict)."""
     from ._lib import BatchLattice, BatchTuning
-    if precision != "single":
-        raise ArgumentError("the batched CG runs FP32 inner iterations")
+    if precision not in ("single", "half"):
+        raise ArgumentError("the batched CG runs FP32 arithmetic on FP32 or int16 fields "
+                            "(precision 'single' or 'half')")
     if not systems:
         raise ArgumentError("no systems")
     lats = (BatchLattice * len(systems))()
@@ -414,7 +416,7 @@ def cg_batched_(systems, *, rtol=1e-10, atol=0.0, maxiter=5000, delta=0.1,
     prm.op = 0
     prm.kappa = 0.0
     prm.rtol, prm.atol, prm.maxiter = float(rtol), float(atol), int(maxiter)
-    prm.precision = PREC["single"]
+    prm.precision = PREC[precision]
     prm.delta = float(delta)
     prm.check_interval = int(check_interval)
     res = (CGResultC * total)()
@@ -431,4 +433,6 @@ def cg_batched_(systems, *, rtol=1e-10, atol=0.0, maxiter=5000, delta=0.1,
                     link_reals=r.link_reals) for r in res]
     return out, dict(rhs_block=tun.rhs_block, threads=tun.threads,
                      ms_per_iteration=tun.ms_per_iteration,
-                     graph_iterations=tun.graph_iterations)
+                     graph_iterations=tun.graph_iterations,
+                     kernel_family=tun.kernel_family,
+                     ms_stencils=tun.ms_stencils)
