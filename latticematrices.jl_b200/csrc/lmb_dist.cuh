@@ -259,6 +259,101 @@ __global__ void __launch_bounds__(kDslashThreads)
 }
 
 // ---------------------------------------------------------------------------
+// int16 boundary slabs of a block split along t only: the two x-adjacent
+// sites of a thread lie in slab t = 0 (TB = 1: the backward t hop reads the
+// minus ghost layer and the ghost link) or t = L_t - 1 (TB = 2: the forward
+// t hop reads the plus ghost layer); the site's index within its slab is its
+// face index.  The other seven hops are the single-lattice ones.
+// ---------------------------------------------------------------------------
+template <int DAG, int PHM, int TB>
+LMB_D void hop_t_ghost(const Geom &g, int s0, const int *c0, const Field<PREC_HALF, 12> &in,
+                       const Field<PREC_HALF, 12> &ghost, const Gauge12<PREC_HALF> &U,
+                       const Gauge12<PREC_HALF> &Ughost, Cx2 *acc) {
+  constexpr int FPM = DAG ? +1 : -1;
+  constexpr int BPM = -FPM;
+  const int f = s0 - c0[3] * g.stride[3];  // index within the slab = face index
+  Cx2 p[12], h[6], uh[6], u[9];
+  float2 nc2;
+  {  // forward: t + 1
+    if constexpr (TB == 2) load_adj_raw(ghost, f, p, nc2);  // the sender applied any phase
+    else load_adj_raw(in, s0 + g.stride[3], p, nc2);
+    project_raw<FPM, 3>(p, nc2, h);
+    load_adj(U, 3, s0, u);
+    su3_mul_half(u, h, uh);
+    reconstruct<FPM, 3>(acc, uh);
+  }
+  {  // backward: t - 1
+    if constexpr (TB == 1) {
+      load_adj_raw(ghost, f, p, nc2);
+      project_raw<BPM, 3>(p, nc2, h);
+      load_adj(Ughost, 3, f, u);
+    } else {
+      load_adj_raw(in, s0 - g.stride[3], p, nc2);
+      project_raw<BPM, 3>(p, nc2, h);
+      load_adj(U, 3, s0 - g.stride[3], u);
+    }
+    su3_adj_mul_half(u, h, uh);
+    reconstruct<BPM, 3>(acc, uh);
+  }
+  (void)PHM;
+}
+
+template <int DAG, bool CLOVER, int PHM, int TB, class CL>
+LMB_D void half_tslab_sites(const Geom &g, int s0, const Field<PREC_HALF, 12> &in,
+                            const Field<PREC_HALF, 12> &ghost, const Gauge12<PREC_HALF> &U,
+                            const Gauge12<PREC_HALF> &Ughost, const CL &A, float kappa, Cx2 *out) {
+  int c0[4], c1[4];
+  site_coords(g, s0, c0);
+  c1[0] = c0[0] + 1;
+  c1[1] = c0[1];
+  c1[2] = c0[2];
+  c1[3] = c0[3];
+#pragma unroll
+  for (int k = 0; k < 12; k++) out[k] = cx2_zero();
+  hop_adj<DAG, 0, PHM>(g, s0, c0, c1, in, U, out);
+  hop_adj<DAG, 1, PHM>(g, s0, c0, c1, in, U, out);
+  hop_adj<DAG, 2, PHM>(g, s0, c0, c1, in, U, out);
+  hop_t_ghost<DAG, PHM, TB>(g, s0, c0, in, ghost, U, Ughost, out);
+  Cx2 p[12];
+  load_adj(in, s0, p);
+  const float2 nk2 = f2(-kappa);
+  if constexpr (CLOVER) {
+#pragma unroll
+    for (int k = 0; k < 12; k++) out[k] = Cx2(nk2 * out[k].re, nk2 * out[k].im);
+    float2 a[36];
+#pragma unroll
+    for (int blk = 0; blk < 2; blk++) {
+      load_adj(A, blk, s0, a);
+      herm6_mul_acc(a, p + 6 * blk, out + 6 * blk);
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 12; k++) out[k] = Cx2(fma2(nk2, out[k].re, p[k].re), fma2(nk2, out[k].im, p[k].im));
+  }
+}
+
+// one thread per x-adjacent pair of the two boundary slabs (pairs
+// [0, F/2) in slab t = 0, [F/2, F) in slab t = L_t - 1; F = L_x L_y L_z)
+template <int DAG, bool CLOVER, int PHM, class CL, class Epi>
+__global__ void __launch_bounds__(kDslashThreads, LMB_PAIR_MINB)
+    wilson_half_tslab_kernel(const Geom g, const Field<PREC_HALF, 12> in, const Field<PREC_HALF, 12> ghm,
+                             const Field<PREC_HALF, 12> ghp, const Gauge12<PREC_HALF> U,
+                             const Gauge12<PREC_HALF> Ughost, const CL A, const float kappa, Epi epi) {
+  if (epi.skip()) return;
+  const int F = g.stride[3], half = F >> 1;
+  const int i = blockIdx.x * kDslashThreads + threadIdx.x;
+  const bool active = i < F;
+  const bool top = i >= half;
+  const int s0 = top ? (int)g.V - F + 2 * (i - half) : 2 * i;
+  Cx2 out[12];
+  if (active) {
+    if (top) half_tslab_sites<DAG, CLOVER, PHM, 2>(g, s0, in, ghp, U, Ughost, A, kappa, out);
+    else half_tslab_sites<DAG, CLOVER, PHM, 1>(g, s0, in, ghm, U, Ughost, A, kappa, out);
+  }
+  epi.pair_adj(s0, active, out);
+}
+
+// ---------------------------------------------------------------------------
 // staggered / HISQ, one site per thread
 // ---------------------------------------------------------------------------
 template <typename R, int MU, int D, int P, class G>

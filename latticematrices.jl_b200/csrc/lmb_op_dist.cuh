@@ -11,6 +11,12 @@
 
 namespace lmb {
 
+// epilogues the x-adjacent pair stencils drive (pair_adj)
+template <class Epi> struct HasPairAdj { static constexpr bool value = false; };
+template <int PS> struct HasPairAdj<EpiStore<PS, 12>> { static constexpr bool value = true; };
+template <int PS> struct HasPairAdj<EpiStoreNorm<PS, 12>> { static constexpr bool value = true; };
+template <int PS, int PX> struct HasPairAdj<EpiCGUpdate<PS, PX, 12>> { static constexpr bool value = true; };
+
 template <int P, int NC>
 int dist_exchange(lmb_ctx *ctx, const Field<P, NC> &in, const DistView &dv, GhostSpinors<P, NC> &gh,
                   cudaStream_t st) {
@@ -138,6 +144,19 @@ struct DistWilsonPolicy {
               g, dv, in, U, A, kappa, e);
         },
         [&](const Epi &e, const int *list, int n) {
+          if constexpr (P == PREC_HALF && std::is_same<G, Gauge12<PREC_HALF>>::value && HasPairAdj<Epi>::value) {
+            // t-only split, x even: the two slabs on the x-adjacent pair stencil
+            if (slab.hi > slab.lo && ctx->pair_sites && ctx->adj_sites && g.L[0] % 2 == 0) {
+              const int F = g.stride[3];
+              if (phase_mode_of(g.phase_mask) == PH_T)
+                wilson_half_tslab_kernel<DAG, CLOVER, PH_T><<<grid_for(F, kDslashThreads), kDslashThreads, 0, st>>>(
+                    g, in, gh.m[3], gh.p[3], U, gu.m[3], A, (float)base.kappa, e);
+              else
+                wilson_half_tslab_kernel<DAG, CLOVER, PH_ANY><<<grid_for(F, kDslashThreads), kDslashThreads, 0, st>>>(
+                    g, in, gh.m[3], gh.p[3], U, gu.m[3], A, (float)base.kappa, e);
+              return;
+            }
+          }
           wilson_boundary_kernel<R, DAG, CLOVER><<<grid_for(n, kDslashThreads), kDslashThreads, 0, st>>>(
               g, dv, in, gh, U, gu, A, kappa, e, list, n);
         });
