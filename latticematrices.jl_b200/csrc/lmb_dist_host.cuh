@@ -42,7 +42,11 @@ struct lmb_dist {
   unsigned split = 0;  // dimensions exchanged with the neighbours
   ncclComm_t comm = nullptr;
   cudaStream_t comm_stream = nullptr;
-  cudaEvent_t ev_packed = nullptr, ev_comm = nullptr;
+  // the boundary kernels run here (higher priority), beside the interior
+  // kernel, with reduction scratch of their own
+  cudaStream_t bnd_stream = nullptr;
+  cudaEvent_t ev_packed = nullptr, ev_comm = nullptr, ev_bnd = nullptr;
+  unsigned *bcounter = nullptr;
   double *sums = nullptr;  // two device doubles: interior and boundary totals
   // boundary sites of the block for each halo depth (device lists)
   std::map<int, std::pair<int *, int>> boundary;

@@ -155,8 +155,11 @@ void dist_release(lmb_ctx *ctx) {
   if (!d) return;
   if (d->comm) nccl_api().CommDestroy(d->comm);
   if (d->comm_stream) cudaStreamDestroy(d->comm_stream);
+  if (d->bnd_stream) cudaStreamDestroy(d->bnd_stream);
   if (d->ev_packed) cudaEventDestroy(d->ev_packed);
   if (d->ev_comm) cudaEventDestroy(d->ev_comm);
+  if (d->ev_bnd) cudaEventDestroy(d->ev_bnd);
+  cudaFree(d->bcounter);
   cudaFree(d->sums);
   for (auto &kv : d->boundary) cudaFree(kv.second.first);
   for (auto &set : d->ghost)
@@ -266,9 +269,15 @@ int lmb_set_process_grid(lmb_ctx *ctx, const void *nccl_id, int nranks, int rank
     dist_release(ctx);
     return fail(ctx, LMB_ERR_CUDA, "ncclCommInitRank: %s", nc.GetErrorString(r));
   }
+  int prio_low = 0, prio_high = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
   if (cudaStreamCreateWithFlags(&d->comm_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&d->bnd_stream, cudaStreamNonBlocking, prio_high) != cudaSuccess ||
       cudaEventCreateWithFlags(&d->ev_packed, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&d->ev_comm, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&d->ev_bnd, cudaEventDisableTiming) != cudaSuccess ||
+      cudaMalloc(&d->bcounter, sizeof(unsigned)) != cudaSuccess ||
+      cudaMemset(d->bcounter, 0, sizeof(unsigned)) != cudaSuccess ||
       cudaMalloc(&d->sums, 2 * sizeof(double)) != cudaSuccess) {
     dist_release(ctx);
     return fail(ctx, LMB_ERR_CUDA, "process-grid resources");

@@ -87,7 +87,10 @@ GhostLinks<G> ghost_views(const lmb_ctx *ctx, int which, const DistView &dv, boo
   return gu;
 }
 
-// interior launch, wait for the faces, boundary launch, sum over the ranks
+// interior launch on `st`; the boundary launch on the boundary stream once
+// the faces have arrived, beside the interior (its blocks take SMs as the
+// interior's retire; separate reduction scratch); then `st` waits for it and
+// the two totals are summed over the ranks
 template <class Epi, class Interior, class Boundary>
 int dist_stencil(lmb_ctx *ctx, int depth, const Epi &epi, cudaStream_t st, Interior interior, Boundary boundary) {
   lmb_dist *d = ctx->dist;
@@ -99,12 +102,24 @@ int dist_stencil(lmb_ctx *ctx, int depth, const Epi &epi, cudaStream_t st, Inter
   if constexpr (ReducingEpi<Epi>::value) {
     e0.local = d->sums;
     e1.local = d->sums + 1;
+    // one slot per block of the boundary launch (at least 32 threads a block)
+    e1.partials = (double *)workspace(ctx, "dist_bpartials", sizeof(double) * grid_for(ctx->g.V, 32));
+    if (!e1.partials) return fail(ctx, LMB_ERR_CUDA, "out of device memory (boundary partials)");
+    e1.counter = d->bcounter;
   }
   interior(e0);
   LMB_CHECK_LAUNCH(ctx);
-  LMB_CUDA(ctx, cudaStreamWaitEvent(st, d->ev_comm, 0));
-  if (n > 0) boundary(e1, list, n);
-  LMB_CHECK_LAUNCH(ctx);
+  if (n > 0) {
+    // the boundary stream's inputs were all produced on `st` before the face
+    // packing, so the arrival of the faces orders it after them
+    LMB_CUDA(ctx, cudaStreamWaitEvent(d->bnd_stream, d->ev_comm, 0));
+    boundary(e1, list, n, d->bnd_stream);
+    LMB_CHECK_LAUNCH(ctx);
+    LMB_CUDA(ctx, cudaEventRecord(d->ev_bnd, d->bnd_stream));
+    LMB_CUDA(ctx, cudaStreamWaitEvent(st, d->ev_bnd, 0));
+  } else {
+    LMB_CUDA(ctx, cudaStreamWaitEvent(st, d->ev_comm, 0));
+  }
   if constexpr (ReducingEpi<Epi>::value) {
     // no split dimension: no boundary kernel, and its total is zero
     if (n == 0) LMB_CUDA(ctx, cudaMemsetAsync(d->sums + 1, 0, sizeof(double), st));
@@ -143,21 +158,21 @@ struct DistWilsonPolicy {
           wilson_interior_kernel<R, DAG, CLOVER, PH_ANY><<<grid_for(g.V, kDslashThreads), kDslashThreads, 0, st>>>(
               g, dv, in, U, A, kappa, e);
         },
-        [&](const Epi &e, const int *list, int n) {
+        [&](const Epi &e, const int *list, int n, cudaStream_t bs) {
           if constexpr (P == PREC_HALF && std::is_same<G, Gauge12<PREC_HALF>>::value && HasPairAdj<Epi>::value) {
             // t-only split, x even: the two slabs on the x-adjacent pair stencil
             if (slab.hi > slab.lo && ctx->pair_sites && ctx->adj_sites && g.L[0] % 2 == 0) {
               const int F = g.stride[3];
               if (phase_mode_of(g.phase_mask) == PH_T)
-                wilson_half_tslab_kernel<DAG, CLOVER, PH_T><<<grid_for(F, kDslashThreads), kDslashThreads, 0, st>>>(
+                wilson_half_tslab_kernel<DAG, CLOVER, PH_T><<<grid_for(F, kDslashThreads), kDslashThreads, 0, bs>>>(
                     g, in, gh.m[3], gh.p[3], U, gu.m[3], A, (float)base.kappa, e);
               else
-                wilson_half_tslab_kernel<DAG, CLOVER, PH_ANY><<<grid_for(F, kDslashThreads), kDslashThreads, 0, st>>>(
+                wilson_half_tslab_kernel<DAG, CLOVER, PH_ANY><<<grid_for(F, kDslashThreads), kDslashThreads, 0, bs>>>(
                     g, in, gh.m[3], gh.p[3], U, gu.m[3], A, (float)base.kappa, e);
               return;
             }
           }
-          wilson_boundary_kernel<R, DAG, CLOVER><<<grid_for(n, kDslashThreads), kDslashThreads, 0, st>>>(
+          wilson_boundary_kernel<R, DAG, CLOVER><<<grid_for(n, kDslashThreads), kDslashThreads, 0, bs>>>(
               g, dv, in, gh, U, gu, A, kappa, e, list, n);
         });
   }
@@ -219,8 +234,8 @@ struct DistStaggeredPolicy {
           staggered_interior_kernel<R, NAIK, PH_ANY><<<grid_for(g.V, kStagThreads), kStagThreads, 0, st>>>(
               g, dv, in, X, Lk, mass, fc, lc, e);
         },
-        [&](const Epi &e, const int *list, int n) {
-          staggered_boundary_kernel<R, NAIK><<<grid_for(n, kStagThreads), kStagThreads, 0, st>>>(
+        [&](const Epi &e, const int *list, int n, cudaStream_t bs) {
+          staggered_boundary_kernel<R, NAIK><<<grid_for(n, kStagThreads), kStagThreads, 0, bs>>>(
               g, dv, in, gh, X, gx, Lk, gl, mass, fc, lc, e, list, n);
         });
   }
