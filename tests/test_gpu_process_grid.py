@@ -185,3 +185,31 @@ def test_process_grid_arguments(lmb):
     with pytest.raises(lmb.ArgumentError):   # grid and communicator sizes differ
         ctx.set_process_grid(nid, 1, 0, (2, 1, 1, 1), (0, 0, 0, 0), (1, 0, 0, 0), (0, 0, 0, 0), (0, 0, 0, 0))
     ctx.set_process_grid(None, 1, 0, (1, 1, 1, 1), (0, 0, 0, 0), (0, 0, 0, 0), (0, 0, 0, 0), (0, 0, 0, 0))
+
+
+@pytest.mark.parametrize("split", [(0, 0, 0, 1), (1, 1, 0, 1)])
+def test_split_block_matches_the_single_lattice_kernels(lmb, orc, split):
+    """The interior / boundary split against the unsplit operator on the same
+    links and field: FP64 to rounding (the same arithmetic in another order
+    at the boundary sites), int16 storage within a tenth of a per-mille
+    (its quantisation step is 2^-15 of a site's largest entry)."""
+    from lmb200._lib import Context
+    L, kappa, csw = (4, 4, 6, 8), 0.1355, 1.0
+    U = orc.random_su3_links(L, 0.25, 11)
+    psi = orc.gaussian_field(L, 3, 4, 12)
+    Ud = _links(lmb, U, 1)
+    pd = lmb.LatticeMatrix.from_array(psi, nw=1, phases=PHASES)
+    st = _stream()
+    whole = Context(0)
+    whole.set_geometry(L, 1, PHASES, (0, 0, 0, 0), 0)
+    whole.upload_links(0, [u.data_ptr() for u in Ud], [u.halo_epoch.core for u in Ud], st)
+    grid = _grid_ctx(lmb, L, 1, PHASES, split)
+    grid.upload_links(0, [u.data_ptr() for u in Ud], [u.halo_epoch.core for u in Ud], st)
+    for dag in (0, 1):
+        for prec, tol in (("double", 1e-14), ("half", 1e-4)):
+            a, b = pd.similar(), pd.similar()
+            for ctx, out in ((whole, a), (grid, b)):
+                ctx.check(ctx.lib.lmb_wilson_clover_apply(ctx.handle, out.data_ptr(), pd.data_ptr(), kappa, csw,
+                                                          dag, PREC[prec], st))
+            err = rd.rel_err(b.gather_matrix(), a.gather_matrix())
+            assert err <= tol, (split, dag, prec, err)
