@@ -454,13 +454,16 @@ __global__ void __launch_bounds__(NT)
 
 // ---------------------------------------------------------------------------
 // x-adjacent pair family (int16 fields, FP32 arithmetic).  Task t of a group
-// is (tile = t / nact, member r = t % nact); a tile is kDslashThreads pairs
-// of x-adjacent sites.  The stencil is the single-lattice one
+// is (tile group = t / nact, member r = t % nact); a tile group is
+// kPairTilesPerTask tiles of kDslashThreads pairs of x-adjacent sites, walked
+// by one block with its norm carried in registers.  The stencil is the single-lattice one
 // (half_adj_sites, Wilson without clover), the epilogue the CG one of
 // EpiStoreNorm / EpiCGUpdate; each task leaves its block's sum in
 // partials[t], and the group's last task sums every member's partials in
 // tile order and takes the scalar steps.
 // ---------------------------------------------------------------------------
+constexpr int kPairTilesPerTask = 8;
+
 LMB_D bool pair_task_done(const BatchGroup &G, int local, double n2, int ntiles, CGState *states, int role) {
   __shared__ double red[kDslashThreads / 32];
   __shared__ bool last;
@@ -511,73 +514,80 @@ __global__ void __launch_bounds__(kDslashThreads, LMB_PAIR_MINB)
     const int gi = find_group(groups, ngroups, task);
     const BatchGroup &G = groups[gi];
     const int local = task - G.first_task;
-    const int tile = local / G.nact, r = local - tile * G.nact;
+    const int tg = local / G.nact, r = local - tg * G.nact;
     const Geom &g = G.g;
-    const int npairs = (int)(g.V >> 1), ntiles = G.ntasks / G.nact;
+    const int npairs = (int)(g.V >> 1), ntg = G.ntasks / G.nact;
     const bool running = ((volatile CGState *)states)[G.state0 + r].status == ST_RUNNING;  // uniform
-    const int i = tile * kDslashThreads + threadIdx.x;
-    const bool active = running && i < npairs;
-    const int s0 = 2 * i;
+    const Field<PREC_HALF, 12> in =
+        ROLE == ROLE_K1 ? bfield<PREC_HALF>(G.p[r], G.pn[r], g.V) : bfield<PREC_HALF>(G.t[r], G.tn[r], g.V);
+    const Gauge12<PREC_HALF> U{G.Uh, g.V, 1.f};
+    const float kappa = (float)G.kappa;
     double n2 = 0.0;
-    if (active) {
-      const Field<PREC_HALF, 12> in =
-          ROLE == ROLE_K1 ? bfield<PREC_HALF>(G.p[r], G.pn[r], g.V) : bfield<PREC_HALF>(G.t[r], G.tn[r], g.V);
-      const Gauge12<PREC_HALF> U{G.Uh, g.V, 1.f};
-      Cx2 out[12];
-      half_adj_sites<DAG, false, PHM>(g, s0, in, U, NoClover{g.V}, (float)G.kappa, out);
-      float2 q = f2(0.f);
-      if (ROLE == ROLE_K1) {
-        store_adj(bfield<PREC_HALF>(G.t[r], G.tn[r], g.V), s0, out);
+#pragma unroll 1
+    for (int tt = 0; tt < kPairTilesPerTask; tt++) {
+      const int i = (tg * kPairTilesPerTask + tt) * kDslashThreads + threadIdx.x;
+      const bool active = running && i < npairs;
+      const int s0 = 2 * i;
+      if (active) {
+        Cx2 out[12];
+        half_adj_sites<DAG, false, PHM>(g, s0, in, U, NoClover{g.V}, kappa, out);
+        float2 q = f2(0.f);
+        if (ROLE == ROLE_K1) {
+          store_adj(bfield<PREC_HALF>(G.t[r], G.tn[r], g.V), s0, out);
 #pragma unroll
-        for (int k = 0; k < 12; k++) q = norm2_acc(out[k], q);
-      } else {
-        const float a = (float)states[G.state0 + r].alpha;
-        const float2 pa = f2(a), na = f2(-a);
-        const Field<PREC_HALF, 12> pf = bfield<PREC_HALF>(G.p[r], G.pn[r], g.V);
-        const Field<PREC_HALF, 12> rf = bfield<PREC_HALF>(G.r[r], G.rn[r], g.V);
-        const Field<PREC_SINGLE, 12> xf{G.xl[r], nullptr, g.V};
-        Cx2 pv[12], rv[12], xv[12];
-        load_adj_rw(pf, s0, pv);
-        load_adj_rw(rf, s0, rv);
-        load_adj_rw(xf, s0, xv);
+          for (int k = 0; k < 12; k++) q = norm2_acc(out[k], q);
+        } else {
+          const float a = (float)states[G.state0 + r].alpha;
+          const float2 pa = f2(a), na = f2(-a);
+          const Field<PREC_HALF, 12> pf = bfield<PREC_HALF>(G.p[r], G.pn[r], g.V);
+          const Field<PREC_HALF, 12> rf = bfield<PREC_HALF>(G.r[r], G.rn[r], g.V);
+          const Field<PREC_SINGLE, 12> xf{G.xl[r], nullptr, g.V};
+          Cx2 pv[12], rv[12], xv[12];
+          load_adj_rw(pf, s0, pv);
+          load_adj_rw(rf, s0, rv);
+          load_adj_rw(xf, s0, xv);
 #pragma unroll
-        for (int k = 0; k < 12; k++) {
-          rv[k] = Cx2(fma2(na, out[k].re, rv[k].re), fma2(na, out[k].im, rv[k].im));
-          xv[k] = Cx2(fma2(pa, pv[k].re, xv[k].re), fma2(pa, pv[k].im, xv[k].im));
-          q = norm2_acc(rv[k], q);
+          for (int k = 0; k < 12; k++) {
+            rv[k] = Cx2(fma2(na, out[k].re, rv[k].re), fma2(na, out[k].im, rv[k].im));
+            xv[k] = Cx2(fma2(pa, pv[k].re, xv[k].re), fma2(pa, pv[k].im, xv[k].im));
+            q = norm2_acc(rv[k], q);
+          }
+          store_adj(rf, s0, rv);
+          store_adj(xf, s0, xv);
         }
-        store_adj(rf, s0, rv);
-        store_adj(xf, s0, xv);
+        n2 += (double)q.x + (double)q.y;
       }
-      n2 = (double)q.x + (double)q.y;
     }
-    pair_task_done(G, local, n2, ntiles, states, ROLE);
+    pair_task_done(G, local, n2, ntg, states, ROLE);
     __syncthreads();  // the next task's status read follows this task's finalize
   }
 }
 
-// K3 of the pair family: p = r + beta p on the task's tile (pairs, 256-bit)
+// K3 of the pair family: p = r + beta p on the task's tile group (pairs, 256-bit)
 __global__ void __launch_bounds__(kDslashThreads)
     batch_half_pair_p_kernel(const BatchGroup *groups, int ngroups, int ntasks_total, const CGState *states) {
   for (int task = blockIdx.x; task < ntasks_total; task += gridDim.x) {
     const int gi = find_group(groups, ngroups, task);
     const BatchGroup &G = groups[gi];
     const int local = task - G.first_task;
-    const int tile = local / G.nact, r = local - tile * G.nact;
+    const int tg = local / G.nact, r = local - tg * G.nact;
     const CGState &st = states[G.state0 + r];
     if (((volatile const CGState *)&st)->status != ST_RUNNING) continue;
-    const int i = tile * kDslashThreads + threadIdx.x;
-    if (i >= (int)(G.g.V >> 1)) continue;
-    const int s0 = 2 * i;
     const float2 beta = f2((float)st.beta);
     const Field<PREC_HALF, 12> pf = bfield<PREC_HALF>(G.p[r], G.pn[r], G.g.V);
     const Field<PREC_HALF, 12> rf = bfield<PREC_HALF>(G.r[r], G.rn[r], G.g.V);
-    Cx2 pv[12], rv[12];
-    load_adj_rw(pf, s0, pv);
-    load_adj_rw(rf, s0, rv);
+#pragma unroll 1
+    for (int tt = 0; tt < kPairTilesPerTask; tt++) {
+      const int i = (tg * kPairTilesPerTask + tt) * kDslashThreads + threadIdx.x;
+      if (i >= (int)(G.g.V >> 1)) break;
+      const int s0 = 2 * i;
+      Cx2 pv[12], rv[12];
+      load_adj_rw(pf, s0, pv);
+      load_adj_rw(rf, s0, rv);
 #pragma unroll
-    for (int k = 0; k < 12; k++) pv[k] = Cx2(fma2(beta, pv[k].re, rv[k].re), fma2(beta, pv[k].im, rv[k].im));
-    store_adj(pf, s0, pv);
+      for (int k = 0; k < 12; k++) pv[k] = Cx2(fma2(beta, pv[k].re, rv[k].re), fma2(beta, pv[k].im, rv[k].im));
+      store_adj(pf, s0, pv);
+    }
   }
 }
 

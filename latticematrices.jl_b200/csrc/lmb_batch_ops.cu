@@ -136,10 +136,12 @@ int build_run(lmb_ctx *ctx, BatchRun &br, int family, int nb, int nt, const std:
       G.U64 = links[l]->d12;
       G.nact = std::min(nb, nrhs[l] - r0);
       G.first_task = task;
-      if (family == 2)  // tasks (tile of kDslashThreads x-adjacent pairs, member)
-        G.ntasks = (int)((G.g.V / 2 + kDslashThreads - 1) / kDslashThreads) * G.nact;
-      else
+      if (family == 2) {  // tasks (group of kPairTilesPerTask tiles of kDslashThreads pairs, member)
+        const int64_t tiles = (G.g.V / 2 + kDslashThreads - 1) / kDslashThreads;
+        G.ntasks = (int)((tiles + kPairTilesPerTask - 1) / kPairTilesPerTask) * G.nact;
+      } else {
         G.ntasks = (int)((G.g.V + nt - 1) / nt);
+      }
       if (phase_mode_of(G.g.phase_mask) != PH_T) br.phase_t = false;
       G.state0 = member_lattice_start[l] + r0;
       G.kappa = kappa[l];
