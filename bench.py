@@ -590,7 +590,8 @@ def run_wilson8(args):
 def run_hisq(args):
     """HISQ smearing (fat7+Lepage, U(3), fat7+Naik) on 48^3x96
     links exp(0.25 i H), then staggered D'D CG at mass 0.01 to 1e-10 with FP32
-    fat/long links and FP64 reliable updates; FP64 CG for comparison."""
+    (and int16) fat/long links and fields, FP64 reliable updates; FP64 CG for
+    comparison."""
     import torch
     import lmb200 as lmb
     L = tuple(int(v) for v in (args.lattice if args.lattice != "32,32,32,64"
@@ -606,7 +607,13 @@ def run_hisq(args):
     x = b.similar()
     out = {"workload": "HISQ smearing + staggered D'D CG, %dx%dx%dx%d, m 0.01" % L,
            "smear_s": t_smear}
-    for prec in ("single", "double"):
+    # algorithmic bytes per site (each link matrix once: 4 fat + 4 Naik x 18
+    # reals; K1 links + in + out, K2 links + in + p + r (rw) + x (rw)):
+    # FP32 / FP64 156 and 180 reals; int16 links 8 x 36 B, spinor 16 B + 4 B
+    # norm, x FP32 24 B
+    kbytes = {"single": (156 * 4, 180 * 4), "double": (156 * 8, 180 * 8),
+              "half": (288 + 2 * 20, 288 + 4 * 20 + 2 * 24)}
+    for prec in ("single", "half", "double"):
         lmb.clear_matrix_(x)
         lmb.cg_(x, A, b, rtol=1e-10, precision=prec, maxiter=args.maxiter)
         lmb.clear_matrix_(x)
@@ -614,18 +621,15 @@ def run_hisq(args):
                                          maxiter=args.maxiter, profile=True), st)
         k1 = res.dslash_ms / max(res.dslash_launches, 1)
         k2 = res.update_ms / max(res.update_launches, 1)
-        rb = 4 if prec == "single" else 8
-        # each link matrix is read once per site (the backward hops reuse the
-        # neighbours' links): 4 fat + 4 Naik x 18 reals = 144 reals.
-        # K1: links + in + out = 156 reals per site;
-        # K2: links + in + p + r (rw) + x (rw) = 180 reals per site
+        b1, b2 = kbytes[prec]
         out[prec] = {"time_s": t, "iterations": res.iterations, "converged": res.converged,
                      "true_rel_residual": res.true_residual_norm / max(1e-300, float(
                          torch.linalg.vector_norm(b.core_view()))),
                      "reliable_updates": res.reliable_updates,
-                     "k1_ms": k1, "k1_gbs": 156 * rb * sites / (k1 * 1e-3) / 1e9,
-                     "k2_ms": k2, "k2_gbs": 180 * rb * sites / (k2 * 1e-3) / 1e9}
+                     "k1_ms": k1, "k1_gbs": b1 * sites / (k1 * 1e-3) / 1e9,
+                     "k2_ms": k2, "k2_gbs": b2 * sites / (k2 * 1e-3) / 1e9}
     out["speedup_single_vs_fp64"] = out["double"]["time_s"] / out["single"]["time_s"]
+    out["speedup_half_vs_fp64"] = out["double"]["time_s"] / out["half"]["time_s"]
     print(json.dumps(out), flush=True)
 
 

@@ -32,8 +32,8 @@ struct StaggeredPolicy {
     const unsigned grid = grid_for(rg.hi - rg.lo, kStagThreads);
     const R fc = (R)(DAG ? -0.5 : 0.5);
     const R lc = (R)(DAG ? (1.0 + eps) / 48.0 : -(1.0 + eps) / 48.0);
-    if constexpr (P == PREC_SINGLE && PHM == PH_T) {
-      // x-adjacent two-site kernel: even x extent, 18-real FP32 links
+    if constexpr ((P == PREC_SINGLE || P == PREC_HALF) && PHM == PH_T) {
+      // x-adjacent two-site kernel: even x extent, 18-real FP32 or int16 links
       const LinkSet &thin = ctx->links[LMB_LINKS_THIN];
       if (ctx->pair_sites && ctx->adj_sites && g.L[0] % 2 == 0 && (naik || !thin.recon(P))) {
         const unsigned grid2 = grid_for((rg.hi - rg.lo) / 2, kStagThreads);
@@ -42,16 +42,16 @@ struct StaggeredPolicy {
           const Gauge<P> Lk = gauge_view<P>(ctx->links[LMB_LINKS_LONG], g.V);
           if constexpr (PersistentEpi<Epi>::value) {
             if (ctx->persistent) {
-              auto kern = staggered_adj_persistent_kernel<true, Epi>;
+              auto kern = staggered_adj_persistent_kernel<true, P, Epi>;
               const unsigned g2 = std::min(grid2, resident_grid(ctx, kern));
               kern<<<g2, kStagThreads, 0, st>>>(g, in, X, Lk, mass, fc, lc, epi, (int)grid2, rg);
               return;
             }
           }
-          staggered_adj_kernel<true><<<grid2, kStagThreads, 0, st>>>(g, in, X, Lk, mass, fc, lc, epi, rg);
+          staggered_adj_kernel<true, P><<<grid2, kStagThreads, 0, st>>>(g, in, X, Lk, mass, fc, lc, epi, rg);
         } else {
           const Gauge<P> X = gauge_view<P>(thin, g.V);
-          staggered_adj_kernel<false><<<grid2, kStagThreads, 0, st>>>(g, in, X, X, mass, fc, lc, epi, rg);
+          staggered_adj_kernel<false, P><<<grid2, kStagThreads, 0, st>>>(g, in, X, X, mass, fc, lc, epi, rg);
         }
         return;
       }

@@ -470,6 +470,18 @@ LMB_D void load_adj(const Clover<PREC_HALF> &A, int blk, int64_t s, float2 *a) {
   a[35] = v1.im;
 }
 
+// 18-real int16 links (one (re, im) int32 word per entry, global scale),
+// adjacent pairs: one 64-bit load per entry
+LMB_D void load_adj(const Gauge<PREC_HALF> &U, int mu, int64_t s, Cx2 *u) {
+  const unsigned y = __float_as_uint(U.scale) >> 16;
+  const float2 negc = f2(-U.scale * 1.00390625f);
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    const int2 t = __ldg(reinterpret_cast<const int2 *>(U.data + (mu * 9 + k) * U.V + s));
+    u[k] = dec_pair2(t.x, t.y, y, y, negc);
+  }
+}
+
 // 3-component FP32 fields (float4 plane + float2 plane) and 18-real FP32
 // links (four float4 planes + one float2 plane per direction), adjacent pairs
 LMB_D float4 as_f4(const int4 &v) { return make_float4(__int_as_float(v.x), __int_as_float(v.y), __int_as_float(v.z), __int_as_float(v.w)); }

@@ -214,8 +214,9 @@ __global__ void __launch_bounds__(kStagThreads, LMB_STAG_PMINB)
 }
 
 // ---------------------------------------------------------------------------
-// FP32 HISQ / staggered stencil on x-adjacent site pairs (s0 = 2i, s1 = s0 + 1)
-// with packed FP32 arithmetic and 256-bit loads (lmb_pair.cuh).  Conditions
+// FP32 / int16-storage HISQ and staggered stencil on x-adjacent site pairs
+// (s0 = 2i, s1 = s0 + 1) with packed FP32 arithmetic and 256-bit loads
+// (lmb_pair.cuh).  Conditions
 // of the PH_T mode (only the t phase, every extent >= 3) and an even x
 // extent; 18-real FP32 links.  eta_mu for mu >= 1 is opposite on the two
 // lanes (x and x + 1).
@@ -240,10 +241,11 @@ LMB_D void phase_t_sel(const Geom &g, int wraps, Cx2 *v) {
   for (int i = 0; i < 3; i++) v[i] = v[i] * f;
 }
 
-// acc += eta [U(x) psi(x + D mu) - U(x - D mu)^+ psi(x - D mu)]
-template <int MU, int D>
-LMB_D void stag_hop_adj(const Geom &g, int s0, const int *c0, const int *c1, const Field<PREC_SINGLE, 3> &in,
-                        const Gauge<PREC_SINGLE> &U, float2 eta, Cx2 *acc) {
+// acc += eta [U(x) psi(x + D mu) - U(x - D mu)^+ psi(x - D mu)]; fields and
+// 18-real links stored as FP32 (PS = PREC_SINGLE) or int16 (PREC_HALF)
+template <int MU, int D, int PS>
+LMB_D void stag_hop_adj(const Geom &g, int s0, const int *c0, const int *c1, const Field<PS, 3> &in,
+                        const Gauge<PS> &U, float2 eta, Cx2 *acc) {
   Cx2 v[3], u[9], o[3];
   int w0, w1;
   if constexpr (MU == 0) {
@@ -275,9 +277,9 @@ LMB_D void stag_hop_adj(const Geom &g, int s0, const int *c0, const int *c1, con
 }
 
 // D psi at the x-adjacent sites s0 (x even) and s0 + 1
-template <bool NAIK>
-LMB_D void stag_adj_sites(const Geom &g, int s0, const Field<PREC_SINGLE, 3> &in, const Gauge<PREC_SINGLE> &X,
-                          const Gauge<PREC_SINGLE> &Lk, float mass, float fc, float lc, Cx2 *out) {
+template <bool NAIK, int PS>
+LMB_D void stag_adj_sites(const Geom &g, int s0, const Field<PS, 3> &in, const Gauge<PS> &X, const Gauge<PS> &Lk,
+                          float mass, float fc, float lc, Cx2 *out) {
   int c0[4], c1[4];
   site_coords(g, s0, c0);
   c1[0] = c0[0] + 1;
@@ -288,19 +290,19 @@ LMB_D void stag_adj_sites(const Geom &g, int s0, const Field<PREC_SINGLE, 3> &in
   const float e1 = (p0 & 1) ? -1.f : 1.f, e2 = (p1 & 1) ? -1.f : 1.f, e3 = (p2 & 1) ? -1.f : 1.f;
   const float2 eta0 = f2(1.f), eta1 = f2(e1, -e1), eta2 = f2(e2, -e2), eta3 = f2(e3, -e3);
   Cx2 fat[3] = {cx2_zero(), cx2_zero(), cx2_zero()};
-  stag_hop_adj<0, 1>(g, s0, c0, c1, in, X, eta0, fat);
-  stag_hop_adj<1, 1>(g, s0, c0, c1, in, X, eta1, fat);
-  stag_hop_adj<2, 1>(g, s0, c0, c1, in, X, eta2, fat);
-  stag_hop_adj<3, 1>(g, s0, c0, c1, in, X, eta3, fat);
+  stag_hop_adj<0, 1, PS>(g, s0, c0, c1, in, X, eta0, fat);
+  stag_hop_adj<1, 1, PS>(g, s0, c0, c1, in, X, eta1, fat);
+  stag_hop_adj<2, 1, PS>(g, s0, c0, c1, in, X, eta2, fat);
+  stag_hop_adj<3, 1, PS>(g, s0, c0, c1, in, X, eta3, fat);
   Cx2 psi[3];
   load_adj(in, s0, psi);
   const float2 m2 = f2(mass), f2c = f2(fc);
   if constexpr (NAIK) {
     Cx2 lng[3] = {cx2_zero(), cx2_zero(), cx2_zero()};
-    stag_hop_adj<0, 3>(g, s0, c0, c1, in, Lk, eta0, lng);
-    stag_hop_adj<1, 3>(g, s0, c0, c1, in, Lk, eta1, lng);
-    stag_hop_adj<2, 3>(g, s0, c0, c1, in, Lk, eta2, lng);
-    stag_hop_adj<3, 3>(g, s0, c0, c1, in, Lk, eta3, lng);
+    stag_hop_adj<0, 3, PS>(g, s0, c0, c1, in, Lk, eta0, lng);
+    stag_hop_adj<1, 3, PS>(g, s0, c0, c1, in, Lk, eta1, lng);
+    stag_hop_adj<2, 3, PS>(g, s0, c0, c1, in, Lk, eta2, lng);
+    stag_hop_adj<3, 3, PS>(g, s0, c0, c1, in, Lk, eta3, lng);
     const float2 l2 = f2(lc);
 #pragma unroll
     for (int k = 0; k < 3; k++)
@@ -315,26 +317,25 @@ LMB_D void stag_adj_sites(const Geom &g, int s0, const Field<PREC_SINGLE, 3> &in
 
 // one thread per pair of the range (rg.lo, rg.hi even).  Epi must provide
 // skip() and pair_adj(s0, active, out[3]).
-template <bool NAIK, class Epi>
+template <bool NAIK, int PS, class Epi>
 __global__ void __launch_bounds__(kStagThreads, LMB_PAIR_MINB)
-    staggered_adj_kernel(const Geom g, const Field<PREC_SINGLE, 3> in, const Gauge<PREC_SINGLE> X,
-                         const Gauge<PREC_SINGLE> Lk, const float mass, const float fc, const float lc, Epi epi,
-                         const SiteRange rg) {
+    staggered_adj_kernel(const Geom g, const Field<PS, 3> in, const Gauge<PS> X, const Gauge<PS> Lk,
+                         const float mass, const float fc, const float lc, Epi epi, const SiteRange rg) {
   if (epi.skip()) return;
   const int i = blockIdx.x * kStagThreads + threadIdx.x;
   const bool active = i < ((rg.hi - rg.lo) >> 1);
   const int s0 = rg.lo + 2 * i;
   Cx2 out[3];
-  if (active) stag_adj_sites<NAIK>(g, s0, in, X, Lk, mass, fc, lc, out);
+  if (active) stag_adj_sites<NAIK, PS>(g, s0, in, X, Lk, mass, fc, lc, out);
   epi.pair_adj(s0, active, out);
 }
 
 // persistent form for the reducing CG epilogues (as the Wilson pair kernel)
-template <bool NAIK, class Epi>
+template <bool NAIK, int PS, class Epi>
 __global__ void __launch_bounds__(kStagThreads, LMB_PAIR_MINB)
-    staggered_adj_persistent_kernel(const Geom g, const Field<PREC_SINGLE, 3> in, const Gauge<PREC_SINGLE> X,
-                                    const Gauge<PREC_SINGLE> Lk, const float mass, const float fc, const float lc,
-                                    Epi epi, int ntiles, const SiteRange rg) {
+    staggered_adj_persistent_kernel(const Geom g, const Field<PS, 3> in, const Gauge<PS> X, const Gauge<PS> Lk,
+                                    const float mass, const float fc, const float lc, Epi epi, int ntiles,
+                                    const SiteRange rg) {
   if (epi.skip()) return;
   double red[1] = {0.0};
   const int npairs = (rg.hi - rg.lo) >> 1;
@@ -343,7 +344,7 @@ __global__ void __launch_bounds__(kStagThreads, LMB_PAIR_MINB)
     const bool active = i < npairs;
     const int s0 = rg.lo + 2 * i;
     Cx2 out[3];
-    if (active) stag_adj_sites<NAIK>(g, s0, in, X, Lk, mass, fc, lc, out);
+    if (active) stag_adj_sites<NAIK, PS>(g, s0, in, X, Lk, mass, fc, lc, out);
     epi.pair_adj_acc(s0, active, out, red);
   }
   epi.finish(red);

@@ -89,12 +89,14 @@ def test_hisq_low_precision(lmb, orc, precision, tol):
     assert rd.rel_err(out.gather_matrix(), ref) <= tol
 
 
+@pytest.mark.parametrize("precision,tol", [("single", 5e-6), ("half", 2e-3)])
 @pytest.mark.parametrize("L,adj", [((8, 8, 4, 8), "1"), ((8, 8, 4, 8), "0"), ((6, 4, 4, 3), "1"),
                                    ((5, 4, 4, 6), "1"), ((4, 6, 8, 4), "1")])
-def test_fp32_two_site_paths(lmb, orc, L, adj, monkeypatch):
-    """FP32 HISQ and staggered (18-real links) with antiperiodic t: an even x
-    extent runs two x-adjacent sites per thread (packed FP32, 256-bit loads)
-    unless LMB_ADJ_SITES=0; an odd x extent runs one site per thread."""
+def test_fp32_two_site_paths(lmb, orc, L, adj, monkeypatch, precision, tol):
+    """FP32- and int16-storage HISQ and staggered (18-real links) with
+    antiperiodic t: an even x extent runs two x-adjacent sites per thread
+    (packed FP32, 256-bit loads) unless LMB_ADJ_SITES=0; an odd x extent runs
+    one site per thread."""
     monkeypatch.setenv("LMB_ADJ_SITES", adj)
     U = orc.random_su3_links(L, 0.25, 7)
     fat, lng = orc.hisq_links_from_thin(U, -0.083)
@@ -104,21 +106,21 @@ def test_fp32_two_site_paths(lmb, orc, L, adj, monkeypatch):
     (pd,) = _dev(lmb, [psi], 3, PHASES)
     out = pd.similar()
     for dag in (False, True):
-        lmb.mul_(out, lmb.adjoint(D) if dag else D, pd, precision="single")
+        lmb.mul_(out, lmb.adjoint(D) if dag else D, pd, precision=precision)
         ref = orc.hisq(fat, lng, psi, 0.05, -0.083, PHASES, dagger=dag)
-        assert rd.rel_err(out.gather_matrix(), ref) <= 5e-6
+        assert rd.rel_err(out.gather_matrix(), ref) <= tol
     # plain staggered on non-unitary links (no reconstruction: 18 reals)
     Un = rd.staggered_test_links(L, 3)
     S = lmb.StaggeredDiracOperator4D(_dev(lmb, Un, 1), 0.07)
     (p1,) = _dev(lmb, [psi], 1, PHASES)
     o1 = p1.similar()
     for dag in (False, True):
-        lmb.mul_(o1, lmb.adjoint(S) if dag else S, p1, precision="single")
+        lmb.mul_(o1, lmb.adjoint(S) if dag else S, p1, precision=precision)
         ref = orc.staggered(Un, psi, 0.07, PHASES, dagger=dag)
-        assert rd.rel_err(o1.gather_matrix(), ref) <= 5e-6
+        assert rd.rel_err(o1.gather_matrix(), ref) <= tol
 
 
-@pytest.mark.parametrize("precision", ["double", "single"])
+@pytest.mark.parametrize("precision", ["double", "single", "half"])
 def test_hisq_cg(lmb, orc, precision):
     L = (8, 8, 8, 8)
     U = orc.random_su3_links(L, 0.25, 1)
