@@ -605,6 +605,7 @@ def run_hisq(args):
     U = lmb.random_su3_links(L, 0.25, 1, nw=3)
     st = torch.cuda.current_stream()
     links, t_smear = _timed(lambda: lmb.hisq_links_from_thin(U, 0.0), st)
+    del links  # the timed call reuses the cached blocks (no cudaMalloc inside)
     links, t_smear = _timed(lambda: lmb.hisq_links_from_thin(U, 0.0), st)
     D = lmb.HISQDiracOperator4D(links, 0.01, 0.0)
     b = lmb.gaussian_fermion(L, 3, 1, 2, nw=3, phases=PHASES)

@@ -5,6 +5,13 @@
 
 namespace lmb {
 
+// epilogues the FP64 pair stencil drives: one site at a time through
+// site_acc(s, active, v[3], red), then finish(red) once per block
+template <class Epi> struct PairSiteAcc { static constexpr bool value = false; };
+template <> struct PairSiteAcc<EpiStore<PREC_DOUBLE, 3>> { static constexpr bool value = true; };
+template <> struct PairSiteAcc<EpiStoreNorm<PREC_DOUBLE, 3>> { static constexpr bool value = true; };
+template <> struct PairSiteAcc<EpiCGUpdate<PREC_DOUBLE, PREC_DOUBLE, 3>> { static constexpr bool value = true; };
+
 struct StaggeredPolicy {
   static constexpr int NC = 3;
   bool naik;  // HISQ: fat links X (LMB_LINKS_FAT) and Naik links L (LMB_LINKS_LONG)
@@ -85,11 +92,38 @@ struct StaggeredPolicy {
     // FP64 HISQ stencils measured faster on B200 with the branch form (PH_ANY).
     return launch_range<P, DAG>(ctx, in, epi, st, whole(ctx->g));
   }
+  // FP64 x-adjacent pair stencil (PH_T, even x extent, 18-real links, an
+  // even range of sites); false when it does not apply
+  template <int DAG, class Epi>
+  bool launch_pair_d(lmb_ctx *ctx, const Field<PREC_DOUBLE, 3> &in, const Epi &epi, cudaStream_t st,
+                     const SiteRange rg) const {
+    const Geom &g = ctx->g;
+    const LinkSet &thin = ctx->links[LMB_LINKS_THIN];
+    if (!ctx->pair_sites || !ctx->adj_sites || g.L[0] % 2 || ((rg.lo | rg.hi) & 1) ||
+        (!naik && thin.recon(PREC_DOUBLE)))
+      return false;
+    const double fc = DAG ? -0.5 : 0.5;
+    const double lc = DAG ? (1.0 + eps) / 48.0 : -(1.0 + eps) / 48.0;
+    const unsigned ntiles = grid_for((rg.hi - rg.lo) / 2, kStagThreads);
+    const Gauge<PREC_DOUBLE> X = gauge_view<PREC_DOUBLE>(naik ? ctx->links[LMB_LINKS_FAT] : thin, g.V);
+    const Gauge<PREC_DOUBLE> Lk = naik ? gauge_view<PREC_DOUBLE>(ctx->links[LMB_LINKS_LONG], g.V) : X;
+    auto kern = naik ? staggered_adj_d_kernel<true, Epi> : staggered_adj_d_kernel<false, Epi>;
+    unsigned grid = ntiles;
+    if (PersistentEpi<Epi>::value && ctx->persistent) grid = std::min(ntiles, resident_grid(ctx, kern));
+    kern<<<grid, kStagThreads, 0, st>>>(g, in, X, Lk, mass, fc, lc, epi, (int)ntiles, rg);
+    return true;
+  }
   template <int P, int DAG, class Epi>
   int launch_range(lmb_ctx *ctx, const Field<P, 3> &in, const Epi &epi, cudaStream_t st, const SiteRange rg) const {
     const int *L = ctx->g.L;
-    if (P != PREC_DOUBLE && phase_mode_of(ctx->g.phase_mask) == PH_T && L[0] >= 3 && L[1] >= 3 && L[2] >= 3 &&
-        L[3] >= 3)
+    const bool pht = phase_mode_of(ctx->g.phase_mask) == PH_T && L[0] >= 3 && L[1] >= 3 && L[2] >= 3 && L[3] >= 3;
+    if constexpr (P == PREC_DOUBLE && PairSiteAcc<Epi>::value) {
+      if (pht && launch_pair_d<DAG>(ctx, in, epi, st, rg)) {
+        LMB_CHECK_LAUNCH(ctx);
+        return LMB_OK;
+      }
+    }
+    if (P != PREC_DOUBLE && pht)
       launch_phm<P, PH_T, DAG>(ctx, in, epi, st, rg);
     else
       launch_phm<P, PH_ANY, DAG>(ctx, in, epi, st, rg);

@@ -21,6 +21,12 @@ LMB_D float2 operator+(float2 a, float2 b) { return __fadd2_rn(a, b); }
 LMB_D float2 operator-(float2 a) { return make_float2(-a.x, -a.y); }
 LMB_D float2 operator-(float2 a, float2 b) { return __fadd2_rn(a, -b); }
 LMB_D float2 operator*(float2 a, float2 b) { return __fmul2_rn(a, b); }
+// double2: two scalar FP64 operations (the FP64 two-site stencils pair the
+// sites for their 256-bit loads; FP64 has no packed arithmetic)
+LMB_D double2 operator+(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+LMB_D double2 operator-(double2 a) { return make_double2(-a.x, -a.y); }
+LMB_D double2 operator-(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+LMB_D double2 operator*(double2 a, double2 b) { return make_double2(a.x * b.x, a.y * b.y); }
 
 namespace lmb {
 
@@ -31,6 +37,12 @@ LMB_D float2 f2(float a, float b) { return make_float2(a, b); }
 LMB_D float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 
 LMB_D Cx2 cx2_zero() { return Cx2(f2(0.f), f2(0.f)); }
+
+typedef Cx<double2> Cd2;
+LMB_D double2 d2(double a) { return make_double2(a, a); }
+LMB_D double2 d2(double a, double b) { return make_double2(a, b); }
+LMB_D double2 fmad2(double2 a, double2 b, double2 c) { return make_double2(fma(a.x, b.x, c.x), fma(a.y, b.y, c.y)); }
+LMB_D Cd2 cd2_zero() { return Cd2(d2(0.0), d2(0.0)); }
 
 // a * b
 LMB_D Cx2 operator*(Cx2 a, Cx2 b) {
@@ -308,6 +320,44 @@ LMB_D void ld256_rw(const int4 *p, int4 &a, int4 &b) {
                : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
                : "l"(p)
                : "memory");
+}
+
+// FP64 fields and 18-real links on two sites: x-adjacent (s even, one
+// 256-bit load per plane) or arbitrary (two 128-bit loads)
+LMB_D void ld256d(const double2 *p, double2 &a, double2 &b) {
+  asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(a.x), "=d"(a.y), "=d"(b.x), "=d"(b.y) : "l"(p));
+}
+template <int NC>
+LMB_D void load_adj(const Field<PREC_DOUBLE, NC> &f, int64_t s, Cd2 *v) {
+#pragma unroll
+  for (int k = 0; k < NC; k++) {
+    double2 a, b;
+    ld256d(f.data + k * f.V + s, a, b);
+    v[k] = Cd2(d2(a.x, b.x), d2(a.y, b.y));
+  }
+}
+template <int NC>
+LMB_D void load2(const Field<PREC_DOUBLE, NC> &f, int64_t s0, int64_t s1, Cd2 *v) {
+#pragma unroll
+  for (int k = 0; k < NC; k++) {
+    const double2 a = __ldg(f.data + k * f.V + s0), b = __ldg(f.data + k * f.V + s1);
+    v[k] = Cd2(d2(a.x, b.x), d2(a.y, b.y));
+  }
+}
+LMB_D void load_adj(const Gauge<PREC_DOUBLE> &U, int mu, int64_t s, Cd2 *u) {
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    double2 a, b;
+    ld256d(U.data + (mu * 9 + k) * U.V + s, a, b);
+    u[k] = Cd2(d2(a.x, b.x), d2(a.y, b.y));
+  }
+}
+LMB_D void load2(const Gauge<PREC_DOUBLE> &U, int mu, int64_t s0, int64_t s1, Cd2 *u) {
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    const double2 a = __ldg(U.data + (mu * 9 + k) * U.V + s0), b = __ldg(U.data + (mu * 9 + k) * U.V + s1);
+    u[k] = Cd2(d2(a.x, b.x), d2(a.y, b.y));
+  }
 }
 
 // own-site fields of the epilogues (read and written by the same kernel)

@@ -132,6 +132,11 @@ struct EpiStore {
   LMB_D void pair_adj(int s0, bool active, const Cx2 *v) const {
     if (active) store_adj(out, s0, v);
   }
+  // the site-by-site interface of the FP64 pair stencils (no reduction)
+  template <typename R> LMB_D void site_acc(int s, bool active, const Cx<R> *v, double (&)[1]) const {
+    if (active) out.store(s, v);
+  }
+  LMB_D void finish(double (&)[1]) const {}
 };
 
 template <int PS, int NC = 12>
@@ -236,6 +241,24 @@ struct EpiCGUpdate {  // K2
     double n2[1] = {0.0};
     pair_adj_acc(s0, active, v, n2);
     finish(n2);
+  }
+  // one site: update and add |r|^2 to red (the FP64 pair stencils)
+  template <typename R> LMB_D void site_acc(int s, bool active, const Cx<R> *v, double (&red)[1]) const {
+    if (active) {
+      const R alpha = (R)st->alpha;
+      Cx<R> pv[NC], rv[NC], xv[NC];
+      p.load(s, pv);
+      r.load(s, rv);
+      x.load(s, xv);
+#pragma unroll
+      for (int k = 0; k < NC; k++) {
+        rv[k] = rv[k] - alpha * v[k];
+        xv[k] = xv[k] + alpha * pv[k];
+      }
+      r.store(s, rv);
+      x.store(s, xv);
+      red[0] += sum_norm2(rv, NC);
+    }
   }
   // persistent kernels: update and add |r|^2 to red; finish() once per block
   LMB_D void pair_adj_acc(int s0, bool active, const Cx2 *v, double (&red)[1]) const {

@@ -166,6 +166,7 @@ LMB_D void stag_site(const Geom &g, int s, const SF &in, const GF &X, const GL &
 }
 
 template <int PS, int NC> struct EpiStore;  // lmb_solver.cuh
+template <int PS, int NC> struct EpiStoreNorm;
 template <int PS, int PX, int NC> struct EpiCGUpdate;
 
 // resident blocks per SM requested from the register allocator: the plain
@@ -346,6 +347,130 @@ __global__ void __launch_bounds__(kStagThreads, LMB_PAIR_MINB)
     Cx2 out[3];
     if (active) stag_adj_sites<NAIK, PS>(g, s0, in, X, Lk, mass, fc, lc, out);
     epi.pair_adj_acc(s0, active, out, red);
+  }
+  epi.finish(red);
+}
+
+// ---------------------------------------------------------------------------
+// FP64 HISQ / staggered stencil on x-adjacent site pairs.  FP64 has no packed
+// arithmetic: the point is the loads.  The one-site FP64 stencil is bound by
+// the latency of its 16 gathers of 12 loads each (long-scoreboard stalls,
+// FP64 pipe ~15 % busy); here one 256-bit load per plane serves both sites
+// of every y, z, t hop and of the site's own links, so each load instruction
+// carries twice the bytes.  Same conditions as the FP32 pair stencil (PH_T,
+// even x extent, 18-real links).
+// ---------------------------------------------------------------------------
+LMB_D void phase_t_sel_d(const Geom &g, int wraps, Cd2 *v) {
+  const double *ph = wraps > 0 ? g.ph_fwd[3] : g.ph_bwd[3];
+  const Cd2 f(d2(wraps ? ph[0] : 1.0), d2(wraps ? ph[1] : 0.0));
+#pragma unroll
+  for (int i = 0; i < 3; i++) v[i] = v[i] * f;
+}
+
+template <int MU, int D>
+LMB_D void stag_hop_adj_d(const Geom &g, int s0, const int *c0, const int *c1, const Field<PREC_DOUBLE, 3> &in,
+                          const Gauge<PREC_DOUBLE> &U, double2 eta, Cd2 *acc) {
+  Cd2 v[3], u[9], o[3];
+  int w0, w1;
+  if constexpr (MU == 0) {
+    const int n0 = shift_site_sel(g, s0, c0, 0, D, &w0), n1 = shift_site_sel(g, s0 + 1, c1, 0, D, &w1);
+    load2(in, n0, n1, v);
+  } else {
+    const int n = (D == 1) ? fwd_site(g, s0, c0, MU, 1, &w0) : shift_site_sel(g, s0, c0, MU, D, &w0);
+    load_adj(in, n, v);
+    if constexpr (MU == 3) phase_t_sel_d(g, w0, v);
+  }
+  load_adj(U, MU, s0, u);
+  su3_mul_vec(u, v, o);
+#pragma unroll
+  for (int i = 0; i < 3; i++) acc[i] = Cd2(fmad2(eta, o[i].re, acc[i].re), fmad2(eta, o[i].im, acc[i].im));
+  if constexpr (MU == 0) {
+    const int n0 = shift_site_sel(g, s0, c0, 0, -D, &w0), n1 = shift_site_sel(g, s0 + 1, c1, 0, -D, &w1);
+    load2(in, n0, n1, v);
+    load2(U, 0, n0, n1, u);
+  } else {
+    const int n = (D == 1) ? bwd_site(g, s0, c0, MU, 1, &w0) : shift_site_sel(g, s0, c0, MU, -D, &w0);
+    if (D == 1 && w0) w0 = -1;
+    load_adj(in, n, v);
+    if constexpr (MU == 3) phase_t_sel_d(g, w0, v);
+    load_adj(U, MU, n, u);
+  }
+  su3_adj_mul_vec(u, v, o);
+#pragma unroll
+  for (int i = 0; i < 3; i++) acc[i] = Cd2(fmad2(-eta, o[i].re, acc[i].re), fmad2(-eta, o[i].im, acc[i].im));
+}
+
+template <bool NAIK>
+LMB_D void stag_adj_sites_d(const Geom &g, int s0, const Field<PREC_DOUBLE, 3> &in, const Gauge<PREC_DOUBLE> &X,
+                            const Gauge<PREC_DOUBLE> &Lk, double mass, double fc, double lc, Cd2 *out) {
+  int c0[4], c1[4];
+  site_coords(g, s0, c0);
+  c1[0] = c0[0] + 1;
+  c1[1] = c0[1];
+  c1[2] = c0[2];
+  c1[3] = c0[3];
+  const int p0 = c0[0] + g.eta_off[0], p1 = p0 + c0[1] + g.eta_off[1], p2 = p1 + c0[2] + g.eta_off[2];
+  const double e1 = (p0 & 1) ? -1.0 : 1.0, e2 = (p1 & 1) ? -1.0 : 1.0, e3 = (p2 & 1) ? -1.0 : 1.0;
+  const double2 eta0 = d2(1.0), eta1 = d2(e1, -e1), eta2 = d2(e2, -e2), eta3 = d2(e3, -e3);
+  Cd2 fat[3] = {cd2_zero(), cd2_zero(), cd2_zero()};
+  stag_hop_adj_d<0, 1>(g, s0, c0, c1, in, X, eta0, fat);
+  stag_hop_adj_d<1, 1>(g, s0, c0, c1, in, X, eta1, fat);
+  stag_hop_adj_d<2, 1>(g, s0, c0, c1, in, X, eta2, fat);
+  stag_hop_adj_d<3, 1>(g, s0, c0, c1, in, X, eta3, fat);
+  const double2 m2 = d2(mass), fc2 = d2(fc);
+  Cd2 psi[3];
+  if constexpr (NAIK) {
+    // fat * fc and the Naik sum share one accumulator; psi comes last
+#pragma unroll
+    for (int k = 0; k < 3; k++) fat[k] = Cd2(fc2 * fat[k].re, fc2 * fat[k].im);
+    const double2 lc2 = d2(lc);
+    const double2 el0 = lc2 * eta0, el1 = lc2 * eta1, el2 = lc2 * eta2, el3 = lc2 * eta3;
+    stag_hop_adj_d<0, 3>(g, s0, c0, c1, in, Lk, el0, fat);
+    stag_hop_adj_d<1, 3>(g, s0, c0, c1, in, Lk, el1, fat);
+    stag_hop_adj_d<2, 3>(g, s0, c0, c1, in, Lk, el2, fat);
+    stag_hop_adj_d<3, 3>(g, s0, c0, c1, in, Lk, el3, fat);
+    load_adj(in, s0, psi);
+#pragma unroll
+    for (int k = 0; k < 3; k++) out[k] = Cd2(fmad2(m2, psi[k].re, fat[k].re), fmad2(m2, psi[k].im, fat[k].im));
+  } else {
+    load_adj(in, s0, psi);
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+      out[k] = Cd2(fmad2(fc2, fat[k].re, m2 * psi[k].re), fmad2(fc2, fat[k].im, m2 * psi[k].im));
+  }
+}
+
+// resident 128-thread blocks per SM requested for the FP64 pair stencil:
+// three (168 registers, a few spilled words) for the plain apply and K2,
+// two (255 registers, no spill) for the persistent K1 (48^3x96 HISQ CG:
+// K1 2.79 against 3.27 ms at three; K2 3.39 against 3.55 ms at two)
+template <class Epi> struct StagD2MinBlocks { static constexpr int value = 3; };
+template <> struct StagD2MinBlocks<EpiStoreNorm<PREC_DOUBLE, 3>> { static constexpr int value = 2; };
+// gridDim.x blocks walk the ntiles tiles of kStagThreads pairs (one tile
+// per block when gridDim.x = ntiles; the resident blocks for the persistent
+// K1), the reduction carried in registers and done once per block
+template <bool NAIK, class Epi>
+__global__ void __launch_bounds__(kStagThreads, StagD2MinBlocks<Epi>::value)
+    staggered_adj_d_kernel(const Geom g, const Field<PREC_DOUBLE, 3> in, const Gauge<PREC_DOUBLE> X,
+                           const Gauge<PREC_DOUBLE> Lk, const double mass, const double fc, const double lc, Epi epi,
+                           int ntiles, const SiteRange rg) {
+  if (epi.skip()) return;
+  double red[1] = {0.0};
+  const int npairs = (rg.hi - rg.lo) >> 1;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int i = tile * kStagThreads + threadIdx.x;
+    const bool active = i < npairs;
+    const int s0 = rg.lo + 2 * i;
+    Cd2 out[3];
+    if (active) stag_adj_sites_d<NAIK>(g, s0, in, X, Lk, mass, fc, lc, out);
+    Cx<double> o0[3], o1[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      o0[k] = Cx<double>(out[k].re.x, out[k].im.x);
+      o1[k] = Cx<double>(out[k].re.y, out[k].im.y);
+    }
+    epi.site_acc(s0, active, o0, red);
+    epi.site_acc(s0 + 1, active, o1, red);
   }
   epi.finish(red);
 }
