@@ -232,6 +232,31 @@ __global__ void __launch_bounds__(kDslashThreads)
   epi(s, active, out);
 }
 
+// The interior of a block split in any dimension on the int16 x-adjacent
+// pair stencil (x extent even): one thread per pair (s0 = 2i, s0 + 1), the
+// pairs with both sites interior; the sites of the other pairs are in the
+// boundary list built with their x partners (dist_boundary, pairs).  An
+// interior site's hops stay inside the block or wrap in place along an
+// unsplit dimension, as on a single lattice.
+template <int DAG, bool CLOVER, int PHM, class CL, class Epi>
+__global__ void __launch_bounds__(kDslashThreads, LMB_PAIR_MINB)
+    wilson_half_adj_interior_kernel(const Geom g, const DistView dv, const Field<PREC_HALF, 12> in,
+                                    const Gauge12<PREC_HALF> U, const CL A, const float kappa, Epi epi) {
+  if (epi.skip()) return;
+  const int s0 = 2 * (blockIdx.x * kDslashThreads + threadIdx.x);
+  bool active = s0 < g.V;
+  if (active) {
+    int c[4];
+    site_coords(g, s0, c);
+    active = dist_interior(g, dv, c);
+    c[0] += 1;
+    active = active && dist_interior(g, dv, c);
+  }
+  Cx2 out[12];
+  if (active) half_adj_sites<DAG, CLOVER, PHM>(g, s0, in, U, A, kappa, out);
+  epi.pair_adj(s0, active, out);
+}
+
 // the sites of `list` (the block's boundary), ghost-aware
 template <typename R, int DAG, bool CLOVER, int P, class G, class CL, class Epi>
 __global__ void __launch_bounds__(kDslashThreads)

@@ -48,7 +48,9 @@ struct lmb_dist {
   cudaEvent_t ev_packed = nullptr, ev_comm = nullptr, ev_bnd = nullptr;
   unsigned *bcounter = nullptr;
   double *sums = nullptr;  // two device doubles: interior and boundary totals
-  // boundary sites of the block for each halo depth (device lists)
+  // boundary sites of the block for each halo depth (device lists; key
+  // 2 depth + 1: with the x partners of boundary sites, for the x-adjacent
+  // pair interior)
   std::map<int, std::pair<int *, int>> boundary;
   // link ghosts per link set and dimension, and what they were built from
   lmb::LinkSet ghost[3][4];
@@ -60,8 +62,10 @@ namespace lmb {
 
 // view of the process grid for a stencil of halo depth `depth`
 DistView dist_view(const lmb_ctx *ctx, int depth);
-// boundary site list of the block for `depth` (built on first use)
-int dist_boundary(lmb_ctx *ctx, int depth, const int **list, int *n);
+// boundary site list of the block for `depth` (built on first use); pairs:
+// also every site whose x partner (x xor 1) is a boundary site, the sites the
+// x-adjacent pair interior leaves out
+int dist_boundary(lmb_ctx *ctx, int depth, bool pairs, const int **list, int *n);
 // ghost links of link set `which` at `depth` layers, in precision prec
 int dist_link_ghosts(lmb_ctx *ctx, int which, int depth, int prec, bool allow_recon, cudaStream_t st);
 // exchange of one field's faces: pack on `st`, NCCL on the communication

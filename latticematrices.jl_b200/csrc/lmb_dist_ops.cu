@@ -61,11 +61,17 @@ DistView dist_view(const lmb_ctx *ctx, int depth) {
   return dv;
 }
 
-int dist_boundary(lmb_ctx *ctx, int depth, const int **list, int *n) {
+int dist_boundary(lmb_ctx *ctx, int depth, bool pairs, const int **list, int *n) {
   lmb_dist *d = ctx->dist;
-  auto it = d->boundary.find(depth);
+  const int key = 2 * depth + (pairs ? 1 : 0);
+  auto it = d->boundary.find(key);
   if (it == d->boundary.end()) {
     const Geom &g = ctx->g;
+    auto on_boundary = [&](const int *c) {
+      for (int mu = 0; mu < 4; mu++)
+        if (((d->split >> mu) & 1) && (c[mu] < depth || c[mu] >= g.L[mu] - depth)) return true;
+      return false;
+    };
     std::vector<int> sites;
     for (int64_t s = 0; s < g.V; s++) {
       int64_t q = s;
@@ -74,9 +80,11 @@ int dist_boundary(lmb_ctx *ctx, int depth, const int **list, int *n) {
         c[mu] = (int)(q % g.L[mu]);
         q /= g.L[mu];
       }
-      bool b = false;
-      for (int mu = 0; mu < 4 && !b; mu++)
-        b = ((d->split >> mu) & 1) && (c[mu] < depth || c[mu] >= g.L[mu] - depth);
+      bool b = on_boundary(c);
+      if (!b && pairs) {
+        int cp[4] = {c[0] ^ 1, c[1], c[2], c[3]};
+        b = cp[0] < g.L[0] && on_boundary(cp);
+      }
       if (b) sites.push_back((int)s);
     }
     int *dev = nullptr;
@@ -84,7 +92,7 @@ int dist_boundary(lmb_ctx *ctx, int depth, const int **list, int *n) {
       LMB_CUDA(ctx, cudaMalloc(&dev, sizeof(int) * sites.size()));
       LMB_CUDA(ctx, cudaMemcpy(dev, sites.data(), sizeof(int) * sites.size(), cudaMemcpyHostToDevice));
     }
-    it = d->boundary.emplace(depth, std::make_pair(dev, (int)sites.size())).first;
+    it = d->boundary.emplace(key, std::make_pair(dev, (int)sites.size())).first;
   }
   *list = it->second.first;
   *n = it->second.second;

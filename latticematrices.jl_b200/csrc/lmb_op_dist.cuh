@@ -91,12 +91,15 @@ GhostLinks<G> ghost_views(const lmb_ctx *ctx, int which, const DistView &dv, boo
 // the faces have arrived, beside the interior (its blocks take SMs as the
 // interior's retire; separate reduction scratch); then `st` waits for it and
 // the two totals are summed over the ranks
+// (pairs: the interior runs on x-adjacent pairs that are wholly interior, so
+// the boundary list also holds the x partners of boundary sites)
 template <class Epi, class Interior, class Boundary>
-int dist_stencil(lmb_ctx *ctx, int depth, const Epi &epi, cudaStream_t st, Interior interior, Boundary boundary) {
+int dist_stencil(lmb_ctx *ctx, int depth, const Epi &epi, cudaStream_t st, Interior interior, Boundary boundary,
+                 bool pairs = false) {
   lmb_dist *d = ctx->dist;
   const int *list = nullptr;
   int n = 0;
-  int rc = dist_boundary(ctx, depth, &list, &n);
+  int rc = dist_boundary(ctx, depth, pairs, &list, &n);
   if (rc) return rc;
   Epi e0 = epi, e1 = epi;
   if constexpr (ReducingEpi<Epi>::value) {
@@ -145,6 +148,11 @@ struct DistWilsonPolicy {
     const Geom g = ctx->g;
     const R kappa = (R)base.kappa;
     const SiteRange slab = t_slab(g, dv);
+    // any other split of an int16 block with even x: the interior on the
+    // x-adjacent pair stencil, pairs with both sites interior
+    bool pairs = false;
+    if constexpr (P == PREC_HALF && std::is_same<G, Gauge12<PREC_HALF>>::value && HasPairAdj<Epi>::value)
+      pairs = slab.hi <= slab.lo && ctx->pair_sites && ctx->adj_sites && g.L[0] % 2 == 0;
     return dist_stencil(
         ctx, 1, epi, st,
         [&](const Epi &e) {
@@ -154,6 +162,18 @@ struct DistWilsonPolicy {
             else
               launch_wilson_cl<P, P, CLOVER, PH_ANY, DAG>(ctx, in, U, A, base.kappa, e, st, slab);
             return;
+          }
+          if constexpr (P == PREC_HALF && std::is_same<G, Gauge12<PREC_HALF>>::value && HasPairAdj<Epi>::value) {
+            if (pairs) {
+              const unsigned grid = grid_for(g.V / 2, kDslashThreads);
+              if (phase_mode_of(g.phase_mask) == PH_T)
+                wilson_half_adj_interior_kernel<DAG, CLOVER, PH_T><<<grid, kDslashThreads, 0, st>>>(
+                    g, dv, in, U, A, (float)base.kappa, e);
+              else
+                wilson_half_adj_interior_kernel<DAG, CLOVER, PH_ANY><<<grid, kDslashThreads, 0, st>>>(
+                    g, dv, in, U, A, (float)base.kappa, e);
+              return;
+            }
           }
           wilson_interior_kernel<R, DAG, CLOVER, PH_ANY><<<grid_for(g.V, kDslashThreads), kDslashThreads, 0, st>>>(
               g, dv, in, U, A, kappa, e);
@@ -174,7 +194,8 @@ struct DistWilsonPolicy {
           }
           wilson_boundary_kernel<R, DAG, CLOVER><<<grid_for(n, kDslashThreads), kDslashThreads, 0, bs>>>(
               g, dv, in, gh, U, gu, A, kappa, e, list, n);
-        });
+        },
+        pairs);
   }
   template <int P, int DAG, class G, class Epi>
   int launch_g(lmb_ctx *ctx, const DistView &dv, const Field<P, 12> &in, const GhostSpinors<P, 12> &gh, const G &U,

@@ -7,8 +7,9 @@ link ghosts from the caller's halo, the all-reduce of every CG reduction --
 and the result must equal the whole-lattice operator and the oracle
 (FP64 <= 1e-13, FP32 storage 5e-6, int16 storage 2e-3).  A block split
 along t only runs its interior slab on the single-lattice kernels (int16
-x-adjacent pairs, persistent reductions); other splits on the one-site
-interior kernel."""
+x-adjacent pairs, persistent reductions); other splits of an int16 block
+with an even x extent run the pairs with both sites interior on the pair
+stencil, and the rest on the one-site interior kernel."""
 import ctypes
 
 import numpy as np
@@ -97,10 +98,14 @@ def _cg(lmb, ctx, op, x, b, prec, **kw):
     return res
 
 
-@pytest.mark.parametrize("split", [(1, 0, 1, 1), (0, 0, 0, 1)])
+# (8, 4, 4, 6) split along x: the int16 interior runs on x-adjacent pairs
+# with both sites interior (x = 2..5), the x partners of the face sites go to
+# the boundary kernel
+@pytest.mark.parametrize("split,L", [((1, 0, 1, 1), (4, 4, 6, 8)), ((0, 0, 0, 1), (4, 4, 6, 8)),
+                                     ((1, 0, 0, 1), (8, 4, 4, 6))])
 @pytest.mark.parametrize("prec", ["double", "single", "half"])
-def test_clover_cg_on_a_split_block(lmb, orc, prec, split):
-    L, kappa, csw = (4, 4, 6, 8), 0.1355, 1.0
+def test_clover_cg_on_a_split_block(lmb, orc, prec, split, L):
+    kappa, csw = 0.1355, 1.0
     U = orc.random_su3_links(L, 0.2, 3)
     b = orc.gaussian_field(L, 3, 4, 4)
     Ud = _links(lmb, U, 1)
@@ -187,14 +192,18 @@ def test_process_grid_arguments(lmb):
     ctx.set_process_grid(None, 1, 0, (1, 1, 1, 1), (0, 0, 0, 0), (0, 0, 0, 0), (0, 0, 0, 0), (0, 0, 0, 0))
 
 
-@pytest.mark.parametrize("split", [(0, 0, 0, 1), (1, 1, 0, 1)])
-def test_split_block_matches_the_single_lattice_kernels(lmb, orc, split):
+@pytest.mark.parametrize("split,L", [((0, 0, 0, 1), (4, 4, 6, 8)), ((1, 1, 0, 1), (4, 4, 6, 8)),
+                                     ((1, 0, 0, 0), (8, 4, 6, 4)), ((1, 1, 0, 1), (8, 4, 6, 4)),
+                                     ((0, 1, 1, 0), (8, 4, 6, 4))])
+def test_split_block_matches_the_single_lattice_kernels(lmb, orc, split, L):
     """The interior / boundary split against the unsplit operator on the same
     links and field: FP64 to rounding (the same arithmetic in another order
     at the boundary sites), int16 storage within a tenth of a per-mille
-    (its quantisation step is 2^-15 of a site's largest entry)."""
+    (its quantisation step is 2^-15 of a site's largest entry).  With an
+    x extent of 8 the int16 interior of any split but t alone runs on
+    x-adjacent pairs, the x split's face partners on the boundary kernel."""
     from lmb200._lib import Context
-    L, kappa, csw = (4, 4, 6, 8), 0.1355, 1.0
+    kappa, csw = 0.1355, 1.0
     U = orc.random_su3_links(L, 0.25, 11)
     psi = orc.gaussian_field(L, 3, 4, 12)
     Ud = _links(lmb, U, 1)
