@@ -238,23 +238,62 @@ __global__ void __launch_bounds__(kDslashThreads)
 // boundary list built with their x partners (dist_boundary, pairs).  An
 // interior site's hops stay inside the block or wrap in place along an
 // unsplit dimension, as on a single lattice.
+// both sites of the x-adjacent pair s0 (x even), s0 + 1 interior
+LMB_D bool pair_interior(const Geom &g, const DistView &dv, int s0) {
+  if (s0 >= g.V) return false;
+  int c[4];
+  site_coords(g, s0, c);
+  if (!dist_interior(g, dv, c)) return false;
+  c[0] += 1;
+  return dist_interior(g, dv, c);
+}
+
 template <int DAG, bool CLOVER, int PHM, class CL, class Epi>
 __global__ void __launch_bounds__(kDslashThreads, LMB_PAIR_MINB)
     wilson_half_adj_interior_kernel(const Geom g, const DistView dv, const Field<PREC_HALF, 12> in,
                                     const Gauge12<PREC_HALF> U, const CL A, const float kappa, Epi epi) {
   if (epi.skip()) return;
   const int s0 = 2 * (blockIdx.x * kDslashThreads + threadIdx.x);
-  bool active = s0 < g.V;
-  if (active) {
-    int c[4];
-    site_coords(g, s0, c);
-    active = dist_interior(g, dv, c);
-    c[0] += 1;
-    active = active && dist_interior(g, dv, c);
-  }
+  const bool active = pair_interior(g, dv, s0);
   Cx2 out[12];
   if (active) half_adj_sites<DAG, CLOVER, PHM>(g, s0, in, U, A, kappa, out);
   epi.pair_adj(s0, active, out);
+}
+
+// The same for the staggered / HISQ stencils (PH_T mode, every extent of the
+// block >= 3, 18-real links): FP32 / int16 storage on packed FP32, and FP64
+// through the epilogue's site_acc / finish
+template <bool NAIK, int PS, class Epi>
+__global__ void __launch_bounds__(kStagThreads, LMB_PAIR_MINB)
+    staggered_adj_interior_kernel(const Geom g, const DistView dv, const Field<PS, 3> in, const Gauge<PS> X,
+                                  const Gauge<PS> Lk, const float mass, const float fc, const float lc, Epi epi) {
+  if (epi.skip()) return;
+  const int s0 = 2 * (blockIdx.x * kStagThreads + threadIdx.x);
+  const bool active = pair_interior(g, dv, s0);
+  Cx2 out[3];
+  if (active) stag_adj_sites<NAIK, PS>(g, s0, in, X, Lk, mass, fc, lc, out);
+  epi.pair_adj(s0, active, out);
+}
+template <bool NAIK, class Epi>
+__global__ void __launch_bounds__(kStagThreads, StagD2MinBlocks<Epi>::value)
+    staggered_adj_d_interior_kernel(const Geom g, const DistView dv, const Field<PREC_DOUBLE, 3> in,
+                                    const Gauge<PREC_DOUBLE> X, const Gauge<PREC_DOUBLE> Lk, const double mass,
+                                    const double fc, const double lc, Epi epi) {
+  if (epi.skip()) return;
+  double red[1] = {0.0};
+  const int s0 = 2 * (blockIdx.x * kStagThreads + threadIdx.x);
+  const bool active = pair_interior(g, dv, s0);
+  Cd2 out[3];
+  if (active) stag_adj_sites_d<NAIK>(g, s0, in, X, Lk, mass, fc, lc, out);
+  Cx<double> o0[3], o1[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    o0[k] = Cx<double>(out[k].re.x, out[k].im.x);
+    o1[k] = Cx<double>(out[k].re.y, out[k].im.y);
+  }
+  epi.site_acc(s0, active, o0, red);
+  epi.site_acc(s0 + 1, active, o1, red);
+  epi.finish(red);
 }
 
 // the sites of `list` (the block's boundary), ghost-aware

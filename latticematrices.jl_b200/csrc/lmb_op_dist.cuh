@@ -221,6 +221,13 @@ struct DistWilsonPolicy {
   bool links_finite(const lmb_ctx *ctx) const { return base.links_finite(ctx); }
 };
 
+// the Naik links of a pair launch, or the fat (thin) ones standing in for the
+// unused slot of plain staggered
+template <int P, class GL> const Gauge<P> &naik_links(const Gauge<P> &X, const GL &Lk) {
+  if constexpr (std::is_same<GL, Gauge<P>>::value) return Lk;
+  else return X;
+}
+
 struct DistStaggeredPolicy {
   static constexpr int NC = 3;
   StaggeredPolicy base;
@@ -245,6 +252,15 @@ struct DistStaggeredPolicy {
     const R fc = (R)(DAG ? -0.5 : 0.5);
     const R lc = (R)(DAG ? (1.0 + base.eps) / 48.0 : -(1.0 + base.eps) / 48.0);
     const SiteRange slab = t_slab(g, dv);
+    // any other split with an even x extent, the t-phase mode and every block
+    // extent >= 3, 18-real links: the interior on the x-adjacent pair stencil
+    // (pairs with both sites interior)
+    constexpr bool pair_ok = std::is_same<GF, Gauge<P>>::value && (!NAIK || std::is_same<GL, Gauge<P>>::value) &&
+                             (P != PREC_DOUBLE || PairSiteAcc<Epi>::value);
+    bool pairs = false;
+    if constexpr (pair_ok)
+      pairs = slab.hi <= slab.lo && ctx->pair_sites && ctx->adj_sites && g.L[0] % 2 == 0 &&
+              phase_mode_of(g.phase_mask) == PH_T && g.L[0] >= 3 && g.L[1] >= 3 && g.L[2] >= 3 && g.L[3] >= 3;
     return dist_stencil(
         ctx, depth(), epi, st,
         [&](const Epi &e) {
@@ -252,13 +268,27 @@ struct DistStaggeredPolicy {
             base.template launch_range<P, DAG>(ctx, in, e, st, slab);
             return;
           }
+          if constexpr (pair_ok) {
+            if (pairs) {
+              const unsigned grid = grid_for(g.V / 2, kStagThreads);
+              const Gauge<P> &L2 = naik_links(X, Lk);  // plain staggered: X in the unused slot
+              if constexpr (P == PREC_DOUBLE)
+                staggered_adj_d_interior_kernel<NAIK><<<grid, kStagThreads, 0, st>>>(g, dv, in, X, L2, mass, fc, lc,
+                                                                                    e);
+              else
+                staggered_adj_interior_kernel<NAIK, P><<<grid, kStagThreads, 0, st>>>(
+                    g, dv, in, X, L2, (float)mass, (float)fc, (float)lc, e);
+              return;
+            }
+          }
           staggered_interior_kernel<R, NAIK, PH_ANY><<<grid_for(g.V, kStagThreads), kStagThreads, 0, st>>>(
               g, dv, in, X, Lk, mass, fc, lc, e);
         },
         [&](const Epi &e, const int *list, int n, cudaStream_t bs) {
           staggered_boundary_kernel<R, NAIK><<<grid_for(n, kStagThreads), kStagThreads, 0, bs>>>(
               g, dv, in, gh, X, gx, Lk, gl, mass, fc, lc, e, list, n);
-        });
+        },
+        pairs);
   }
   template <int P, int DAG, class Epi>
   int launch(lmb_ctx *ctx, const Field<P, 3> &in, const Epi &epi, cudaStream_t st) const {

@@ -128,7 +128,11 @@ def test_clover_cg_on_a_split_block(lmb, orc, prec, split, L):
 @pytest.mark.parametrize("split,L,phases", [((1, 1, 1, 1), (6, 4, 6, 6), TWISTED),
                                             ((0, 0, 1, 1), (6, 4, 6, 6), TWISTED),
                                             ((0, 0, 0, 1), (4, 4, 4, 8), TWISTED),
-                                            ((0, 0, 0, 1), (4, 4, 4, 8), PHASES)])
+                                            ((0, 0, 0, 1), (4, 4, 4, 8), PHASES),
+                                            # t phase only, x extent 10: the interior on x-adjacent
+                                            # pairs (x = 4, 5 with both sites interior at depth 3)
+                                            ((1, 0, 0, 0), (10, 4, 4, 6), PHASES),
+                                            ((1, 0, 1, 1), (10, 4, 8, 8), PHASES)])
 def test_hisq_on_a_split_block_matches_oracle(lmb, orc, split, L, phases):
     mass, eps = 0.05, -0.083
     U = orc.random_su3_links(L, 0.25, 5)
@@ -148,10 +152,10 @@ def test_hisq_on_a_split_block_matches_oracle(lmb, orc, split, L, phases):
                                              PREC[prec], st))
             err = rd.rel_err(out.gather_matrix(), ref)
             assert err <= tol, (split, dag, prec, err)
-    # and the CG on the block, FP64 and FP32 inner iterations
+    # and the CG on the block, FP64 and FP32 / int16 inner iterations
     bd = lmb.LatticeMatrix.from_array(psi, nw=3, phases=phases)
     op = orc.Operator(orc.OP_HISQ, list(X) + list(Ln), L, phases=phases, mass=mass, naik_epsilon=eps)
-    for prec in ("double", "single"):
+    for prec in ("double", "single", "half"):
         x = bd.similar()
         res = _cg(lmb, ctx, 3, x, bd, prec, mass=mass, eps=eps)
         assert res.converged, (prec, res.iterations)
