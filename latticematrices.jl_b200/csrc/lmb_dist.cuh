@@ -396,6 +396,127 @@ LMB_D void half_tslab_sites(const Geom &g, int s0, const Field<PREC_HALF, 12> &i
   }
 }
 
+// Two int16 sites held in two fields or link sets (lane 0: the first at i0,
+// lane 1: the second at i1), for the face pairs whose one site reads a ghost
+LMB_D void load2_raw_ff(const Field<PREC_HALF, 12> &f0, int64_t i0, const Field<PREC_HALF, 12> &f1, int64_t i1,
+                        Cx2 *v, float2 &nc2) {
+  const float b0 = __ldg(f0.norm + i0), b1 = __ldg(f1.norm + i1);
+  const unsigned y0 = __float_as_uint(b0) >> 16, y1 = __float_as_uint(b1) >> 16;
+  nc2 = make_float2(-b0 * 2.0078125f, -b1 * 2.0078125f);
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const int4 t0 = __ldg(f0.data + k * f0.V + i0), t1 = __ldg(f1.data + k * f1.V + i1);
+    const int w0[4] = {t0.x, t0.y, t0.z, t0.w}, w1[4] = {t1.x, t1.y, t1.z, t1.w};
+#pragma unroll
+    for (int j = 0; j < 4; j++) v[4 * k + j] = raw_pair2(w0[j], w1[j], y0, y1);
+  }
+}
+LMB_D void load2_gg(const Gauge12<PREC_HALF> &U0, int64_t i0, const Gauge12<PREC_HALF> &U1, int64_t i1, int mu,
+                    Cx2 *u) {
+  const int q0 = mu * 6, p0 = q0 >> 2, lane0 = q0 & 3;
+  const int4 a0 = __ldg(U0.data + p0 * U0.V + i0), b0 = __ldg(U0.data + (p0 + 1) * U0.V + i0);
+  const int4 a1 = __ldg(U1.data + p0 * U1.V + i1), b1 = __ldg(U1.data + (p0 + 1) * U1.V + i1);
+  const int w0[8] = {a0.x, a0.y, a0.z, a0.w, b0.x, b0.y, b0.z, b0.w};
+  const int w1[8] = {a1.x, a1.y, a1.z, a1.w, b1.x, b1.y, b1.z, b1.w};
+  const float2 negc = f2(-257.0f);  // base 2^8
+#pragma unroll
+  for (int e = 0; e < 6; e++)
+    u[(e / 3) + 3 * (e % 3)] = dec_pair2(w0[lane0 + e], w1[lane0 + e], 0x4380u, 0x4380u, negc);
+  su3_third_row(u);
+}
+
+// x hop of a face pair of a block split along x alone (depth 1): XB = 1 the
+// pair (0, 1), whose site 0 reads its x - 1 neighbour from the minus ghost
+// layer and that neighbour's link from the link ghost; XB = 2 the pair
+// (L_x - 2, L_x - 1), whose site L_x - 1 reads x + 1 from the plus ghost
+// layer.  f = the row's face index; the sender applied any boundary phase.
+template <int DAG, int XB>
+LMB_D void hop_x_ghost(int s0, int f, const Field<PREC_HALF, 12> &in, const Field<PREC_HALF, 12> &ghost,
+                       const Gauge12<PREC_HALF> &U, const Gauge12<PREC_HALF> &Ughost, Cx2 *acc) {
+  constexpr int FPM = DAG ? +1 : -1;
+  constexpr int BPM = -FPM;
+  Cx2 p[12], h[6], uh[6], u[9];
+  float2 nc2;
+  {  // forward: x + 1
+    if constexpr (XB == 2) load2_raw_ff(in, s0 + 1, ghost, f, p, nc2);
+    else load2_raw(in, s0 + 1, s0 + 2, p, nc2);
+    project_raw<FPM, 0>(p, nc2, h);
+    load_adj(U, 0, s0, u);
+    su3_mul_half(u, h, uh);
+    reconstruct<FPM, 0>(acc, uh);
+  }
+  {  // backward: x - 1
+    if constexpr (XB == 1) {
+      load2_raw_ff(ghost, f, in, s0, p, nc2);
+      project_raw<BPM, 0>(p, nc2, h);
+      load2_gg(Ughost, f, U, s0, 0, u);
+    } else {
+      load2_raw(in, s0 - 1, s0, p, nc2);
+      project_raw<BPM, 0>(p, nc2, h);
+      load2(U, 0, s0 - 1, s0, u);
+    }
+    su3_adj_mul_half(u, h, uh);
+    reconstruct<BPM, 0>(acc, uh);
+  }
+}
+
+template <int DAG, bool CLOVER, int PHM, int XB, class CL>
+LMB_D void half_xface_sites(const Geom &g, int s0, int f, const Field<PREC_HALF, 12> &in,
+                            const Field<PREC_HALF, 12> &ghost, const Gauge12<PREC_HALF> &U,
+                            const Gauge12<PREC_HALF> &Ughost, const CL &A, float kappa, Cx2 *out) {
+  int c0[4], c1[4];
+  site_coords(g, s0, c0);
+  c1[0] = c0[0] + 1;
+  c1[1] = c0[1];
+  c1[2] = c0[2];
+  c1[3] = c0[3];
+#pragma unroll
+  for (int k = 0; k < 12; k++) out[k] = cx2_zero();
+  hop_x_ghost<DAG, XB>(s0, f, in, ghost, U, Ughost, out);
+  hop_adj<DAG, 1, PHM>(g, s0, c0, c1, in, U, out);
+  hop_adj<DAG, 2, PHM>(g, s0, c0, c1, in, U, out);
+  hop_adj<DAG, 3, PHM>(g, s0, c0, c1, in, U, out);
+  Cx2 p[12];
+  load_adj(in, s0, p);
+  const float2 nk2 = f2(-kappa);
+  if constexpr (CLOVER) {
+#pragma unroll
+    for (int k = 0; k < 12; k++) out[k] = Cx2(nk2 * out[k].re, nk2 * out[k].im);
+    float2 a[36];
+#pragma unroll
+    for (int blk = 0; blk < 2; blk++) {
+      load_adj(A, blk, s0, a);
+      herm6_mul_acc(a, p + 6 * blk, out + 6 * blk);
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 12; k++) out[k] = Cx2(fma2(nk2, out[k].re, p[k].re), fma2(nk2, out[k].im, p[k].im));
+  }
+}
+
+// one thread per face pair of a block split along x alone, x extent even and
+// >= 4: threads [0, F) the pairs (0, 1) of the F = L_y L_z L_t rows (face
+// index = row), [F, 2F) the pairs (L_x - 2, L_x - 1)
+template <int DAG, bool CLOVER, int PHM, class CL, class Epi>
+__global__ void __launch_bounds__(kDslashThreads, LMB_PAIR_MINB)
+    wilson_half_xface_kernel(const Geom g, const Field<PREC_HALF, 12> in, const Field<PREC_HALF, 12> ghm,
+                             const Field<PREC_HALF, 12> ghp, const Gauge12<PREC_HALF> U,
+                             const Gauge12<PREC_HALF> Ughost, const CL A, const float kappa, Epi epi) {
+  if (epi.skip()) return;
+  const int Lx = g.L[0], F = (int)(g.V / Lx);
+  const int i = blockIdx.x * kDslashThreads + threadIdx.x;
+  const bool active = i < 2 * F;
+  const bool top = i >= F;
+  const int f = top ? i - F : i;
+  const int s0 = f * Lx + (top ? Lx - 2 : 0);
+  Cx2 out[12];
+  if (active) {
+    if (top) half_xface_sites<DAG, CLOVER, PHM, 2>(g, s0, f, in, ghp, U, Ughost, A, kappa, out);
+    else half_xface_sites<DAG, CLOVER, PHM, 1>(g, s0, f, in, ghm, U, Ughost, A, kappa, out);
+  }
+  epi.pair_adj(s0, active, out);
+}
+
 // one thread per x-adjacent pair of the two boundary slabs (pairs
 // [0, F/2) in slab t = 0, [F/2, F) in slab t = L_t - 1; F = L_x L_y L_z)
 template <int DAG, bool CLOVER, int PHM, class CL, class Epi>

@@ -191,6 +191,17 @@ struct DistWilsonPolicy {
                     g, in, gh.m[3], gh.p[3], U, gu.m[3], A, (float)base.kappa, e);
               return;
             }
+            // x-only split, x extent >= 4: its boundary is the two face pairs of every row
+            if (pairs && dv.split == 1u && g.L[0] >= 4) {
+              const unsigned grid = grid_for(2 * (g.V / g.L[0]), kDslashThreads);
+              if (phase_mode_of(g.phase_mask) == PH_T)
+                wilson_half_xface_kernel<DAG, CLOVER, PH_T><<<grid, kDslashThreads, 0, bs>>>(
+                    g, in, gh.m[0], gh.p[0], U, gu.m[0], A, (float)base.kappa, e);
+              else
+                wilson_half_xface_kernel<DAG, CLOVER, PH_ANY><<<grid, kDslashThreads, 0, bs>>>(
+                    g, in, gh.m[0], gh.p[0], U, gu.m[0], A, (float)base.kappa, e);
+              return;
+            }
           }
           wilson_boundary_kernel<R, DAG, CLOVER><<<grid_for(n, kDslashThreads), kDslashThreads, 0, bs>>>(
               g, dv, in, gh, U, gu, A, kappa, e, list, n);

@@ -55,7 +55,9 @@ def _stream():
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
-@pytest.mark.parametrize("split", [(1, 0, 0, 1), (1, 1, 1, 1), (0, 1, 0, 0), (0, 0, 0, 1)])
+# (1, 0, 0, 0): x alone, whose int16 boundary is the two face pairs of every
+# row on the pair stencil (here every site: x extent 4)
+@pytest.mark.parametrize("split", [(1, 0, 0, 1), (1, 1, 1, 1), (0, 1, 0, 0), (0, 0, 0, 1), (1, 0, 0, 0)])
 @pytest.mark.parametrize("clover", [False, True])
 def test_wilson_on_a_split_block_matches_oracle(lmb, orc, split, clover):
     L, kappa, csw = (4, 6, 4, 8), 0.1355, 1.0
@@ -102,7 +104,7 @@ def _cg(lmb, ctx, op, x, b, prec, **kw):
 # with both sites interior (x = 2..5), the x partners of the face sites go to
 # the boundary kernel
 @pytest.mark.parametrize("split,L", [((1, 0, 1, 1), (4, 4, 6, 8)), ((0, 0, 0, 1), (4, 4, 6, 8)),
-                                     ((1, 0, 0, 1), (8, 4, 4, 6))])
+                                     ((1, 0, 0, 1), (8, 4, 4, 6)), ((1, 0, 0, 0), (8, 4, 4, 6))])
 @pytest.mark.parametrize("prec", ["double", "single", "half"])
 def test_clover_cg_on_a_split_block(lmb, orc, prec, split, L):
     kappa, csw = 0.1355, 1.0
