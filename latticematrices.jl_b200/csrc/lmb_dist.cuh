@@ -35,6 +35,10 @@ struct DistView {
   int depth;        // ghost layers
   int face[4];      // F_mu
   int fstr[4][4];   // stride of dimension nu in the face index of dimension mu (0 for nu == mu)
+  // the box of x-adjacent pairs with both sites interior: pair index px (x =
+  // 2 px) in [plo[0], plo[0] + pn[0]), coordinate mu >= 1 in [plo, plo + pn)
+  int plo[4], pn[4];
+  int npairs;
 };
 
 LMB_D int face_index(const DistView &dv, const int *c, int mu) {
@@ -238,14 +242,16 @@ __global__ void __launch_bounds__(kDslashThreads)
 // boundary list built with their x partners (dist_boundary, pairs).  An
 // interior site's hops stay inside the block or wrap in place along an
 // unsplit dimension, as on a single lattice.
-// both sites of the x-adjacent pair s0 (x even), s0 + 1 interior
-LMB_D bool pair_interior(const Geom &g, const DistView &dv, int s0) {
-  if (s0 >= g.V) return false;
-  int c[4];
-  site_coords(g, s0, c);
-  if (!dist_interior(g, dv, c)) return false;
-  c[0] += 1;
-  return dist_interior(g, dv, c);
+// site s0 (x even) of the i-th pair of the interior pair box (i < npairs):
+// the interior kernels run one thread per interior pair, no thread idle
+LMB_D int interior_pair_site(const Geom &g, const DistView &dv, int i) {
+  const int px = dv.plo[0] + i % dv.pn[0];
+  int q = i / dv.pn[0];
+  const int y = dv.plo[1] + q % dv.pn[1];
+  q /= dv.pn[1];
+  const int z = dv.plo[2] + q % dv.pn[2];
+  const int t = dv.plo[3] + q / dv.pn[2];
+  return 2 * px + g.stride[1] * y + g.stride[2] * z + g.stride[3] * t;
 }
 
 template <int DAG, bool CLOVER, int PHM, class CL, class Epi>
@@ -253,8 +259,9 @@ __global__ void __launch_bounds__(kDslashThreads, LMB_PAIR_MINB)
     wilson_half_adj_interior_kernel(const Geom g, const DistView dv, const Field<PREC_HALF, 12> in,
                                     const Gauge12<PREC_HALF> U, const CL A, const float kappa, Epi epi) {
   if (epi.skip()) return;
-  const int s0 = 2 * (blockIdx.x * kDslashThreads + threadIdx.x);
-  const bool active = pair_interior(g, dv, s0);
+  const int i = blockIdx.x * kDslashThreads + threadIdx.x;
+  const bool active = i < dv.npairs;
+  const int s0 = active ? interior_pair_site(g, dv, i) : 0;
   Cx2 out[12];
   if (active) half_adj_sites<DAG, CLOVER, PHM>(g, s0, in, U, A, kappa, out);
   epi.pair_adj(s0, active, out);
@@ -268,8 +275,9 @@ __global__ void __launch_bounds__(kStagThreads, LMB_PAIR_MINB)
     staggered_adj_interior_kernel(const Geom g, const DistView dv, const Field<PS, 3> in, const Gauge<PS> X,
                                   const Gauge<PS> Lk, const float mass, const float fc, const float lc, Epi epi) {
   if (epi.skip()) return;
-  const int s0 = 2 * (blockIdx.x * kStagThreads + threadIdx.x);
-  const bool active = pair_interior(g, dv, s0);
+  const int i = blockIdx.x * kStagThreads + threadIdx.x;
+  const bool active = i < dv.npairs;
+  const int s0 = active ? interior_pair_site(g, dv, i) : 0;
   Cx2 out[3];
   if (active) stag_adj_sites<NAIK, PS>(g, s0, in, X, Lk, mass, fc, lc, out);
   epi.pair_adj(s0, active, out);
@@ -281,8 +289,9 @@ __global__ void __launch_bounds__(kStagThreads, StagD2MinBlocks<Epi>::value)
                                     const double fc, const double lc, Epi epi) {
   if (epi.skip()) return;
   double red[1] = {0.0};
-  const int s0 = 2 * (blockIdx.x * kStagThreads + threadIdx.x);
-  const bool active = pair_interior(g, dv, s0);
+  const int i = blockIdx.x * kStagThreads + threadIdx.x;
+  const bool active = i < dv.npairs;
+  const int s0 = active ? interior_pair_site(g, dv, i) : 0;
   Cd2 out[3];
   if (active) stag_adj_sites_d<NAIK>(g, s0, in, X, Lk, mass, fc, lc, out);
   Cx<double> o0[3], o1[3];

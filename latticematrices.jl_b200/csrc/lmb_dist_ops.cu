@@ -2,6 +2,7 @@
 // communicator of a context (lmb_set_process_grid), ghost links and boundary
 // lists, the all-reduce of the partial sums and F_mu_nu of a block.  The
 // operator drivers are instantiated per precision in lmb_dist_{d,s,h}.cu.
+#include <algorithm>
 #include <dlfcn.h>
 
 #include "lmb_op_dist.cuh"
@@ -58,6 +59,14 @@ DistView dist_view(const lmb_ctx *ctx, int depth) {
       stride *= g.L[nu];
     }
   }
+  int64_t np = 1;
+  for (int mu = 0; mu < 4; mu++) {
+    const int lo = ((dv.split >> mu) & 1) ? depth : 0, hi = g.L[mu] - lo;
+    dv.plo[mu] = mu == 0 ? (lo + 1) / 2 : lo;
+    dv.pn[mu] = std::max(0, mu == 0 ? hi / 2 - dv.plo[0] : hi - lo);
+    np *= dv.pn[mu];
+  }
+  dv.npairs = (int)np;
   return dv;
 }
 

@@ -165,7 +165,8 @@ struct DistWilsonPolicy {
           }
           if constexpr (P == PREC_HALF && std::is_same<G, Gauge12<PREC_HALF>>::value && HasPairAdj<Epi>::value) {
             if (pairs) {
-              const unsigned grid = grid_for(g.V / 2, kDslashThreads);
+              // one block at least: a reducing epilogue writes its (zero) block total
+              const unsigned grid = std::max(1u, (unsigned)grid_for(dv.npairs, kDslashThreads));
               if (phase_mode_of(g.phase_mask) == PH_T)
                 wilson_half_adj_interior_kernel<DAG, CLOVER, PH_T><<<grid, kDslashThreads, 0, st>>>(
                     g, dv, in, U, A, (float)base.kappa, e);
@@ -281,7 +282,8 @@ struct DistStaggeredPolicy {
           }
           if constexpr (pair_ok) {
             if (pairs) {
-              const unsigned grid = grid_for(g.V / 2, kStagThreads);
+              // one block at least: a reducing epilogue writes its (zero) block total
+              const unsigned grid = std::max(1u, (unsigned)grid_for(dv.npairs, kStagThreads));
               const Gauge<P> &L2 = naik_links(X, Lk);  // plain staggered: X in the unused slot
               if constexpr (P == PREC_DOUBLE)
                 staggered_adj_d_interior_kernel<NAIK><<<grid, kStagThreads, 0, st>>>(g, dv, in, X, L2, mass, fc, lc,
