@@ -39,6 +39,9 @@ struct DistView {
   // 2 px) in [plo[0], plo[0] + pn[0]), coordinate mu >= 1 in [plo, plo + pn)
   int plo[4], pn[4];
   int npairs;
+  // the box of interior sites: coordinate mu in [slo, slo + sn)
+  int slo[4], sn[4];
+  int nsites;
 };
 
 LMB_D int face_index(const DistView &dv, const int *c, int mu) {
@@ -60,6 +63,17 @@ LMB_D bool dist_interior(const Geom &g, const DistView &dv, const int *c) {
   for (int mu = 0; mu < 4; mu++)
     if (((dv.split >> mu) & 1) && (c[mu] < dv.depth || c[mu] >= g.L[mu] - dv.depth)) return false;
   return true;
+}
+
+// the i-th site of the interior box (i < nsites) and its coordinates c
+LMB_D int interior_site(const Geom &g, const DistView &dv, int i, int *c) {
+  c[0] = dv.slo[0] + i % dv.sn[0];
+  int q = i / dv.sn[0];
+  c[1] = dv.slo[1] + q % dv.sn[1];
+  q /= dv.sn[1];
+  c[2] = dv.slo[2] + q % dv.sn[2];
+  c[3] = dv.slo[3] + q / dv.sn[2];
+  return c[0] + g.stride[1] * c[1] + g.stride[2] * c[2] + g.stride[3] * c[3];
 }
 
 // the interior of a block split along t only as one range of sites,
@@ -224,14 +238,11 @@ __global__ void __launch_bounds__(kDslashThreads)
     wilson_interior_kernel(const Geom g, const DistView dv, const Field<P, 12> in, const G U, const CL A,
                            const R kappa, Epi epi) {
   if (epi.skip()) return;
-  const int s = blockIdx.x * kDslashThreads + threadIdx.x;
-  bool active = s < g.V;
+  const int i = blockIdx.x * kDslashThreads + threadIdx.x;
+  const bool active = i < dv.nsites;
   Cx<R> out[12];
   int c[4];
-  if (active) {
-    site_coords(g, s, c);
-    active = dist_interior(g, dv, c);
-  }
+  const int s = active ? interior_site(g, dv, i, c) : 0;
   if (active) wilson_site_out<R, DAG, CLOVER, PHM>(g, s, c, in, U, A, kappa, out);
   epi(s, active, out);
 }
@@ -574,14 +585,11 @@ __global__ void __launch_bounds__(kStagThreads)
     staggered_interior_kernel(const Geom g, const DistView dv, const Field<P, 3> in, const GF X, const GL Lk,
                               const R mass, const R fc, const R lc, Epi epi) {
   if (epi.skip()) return;
-  const int s = blockIdx.x * kStagThreads + threadIdx.x;
-  bool active = s < g.V;
+  const int i = blockIdx.x * kStagThreads + threadIdx.x;
+  const bool active = i < dv.nsites;
   Cx<R> out[3];
-  if (active) {
-    int c[4];
-    site_coords(g, s, c);
-    active = dist_interior(g, dv, c);
-  }
+  int c[4];
+  const int s = active ? interior_site(g, dv, i, c) : 0;
   if (active) stag_site<R, NAIK, PHM>(g, s, in, X, Lk, mass, fc, lc, out);
   epi(s, active, out);
 }

@@ -67,6 +67,14 @@ DistView dist_view(const lmb_ctx *ctx, int depth) {
     np *= dv.pn[mu];
   }
   dv.npairs = (int)np;
+  int64_t ns = 1;
+  for (int mu = 0; mu < 4; mu++) {
+    const int lo = ((dv.split >> mu) & 1) ? depth : 0;
+    dv.slo[mu] = lo;
+    dv.sn[mu] = std::max(0, g.L[mu] - 2 * lo);
+    ns *= dv.sn[mu];
+  }
+  dv.nsites = (int)ns;
   return dv;
 }
 

@@ -176,7 +176,8 @@ struct DistWilsonPolicy {
               return;
             }
           }
-          wilson_interior_kernel<R, DAG, CLOVER, PH_ANY><<<grid_for(g.V, kDslashThreads), kDslashThreads, 0, st>>>(
+          wilson_interior_kernel<R, DAG, CLOVER, PH_ANY>
+              <<<std::max(1u, grid_for(dv.nsites, kDslashThreads)), kDslashThreads, 0, st>>>(
               g, dv, in, U, A, kappa, e);
         },
         [&](const Epi &e, const int *list, int n, cudaStream_t bs) {
@@ -294,7 +295,8 @@ struct DistStaggeredPolicy {
               return;
             }
           }
-          staggered_interior_kernel<R, NAIK, PH_ANY><<<grid_for(g.V, kStagThreads), kStagThreads, 0, st>>>(
+          staggered_interior_kernel<R, NAIK, PH_ANY>
+              <<<std::max(1u, grid_for(dv.nsites, kStagThreads)), kStagThreads, 0, st>>>(
               g, dv, in, X, Lk, mass, fc, lc, e);
         },
         [&](const Epi &e, const int *list, int n, cudaStream_t bs) {
